@@ -1,0 +1,247 @@
+/*
+ * tnbp_b200 — C ABI of the B200 (sm_100a) loopy-BP PEPS expectation-value
+ * engine.  Plain C: opaque handles, plain pointers and sizes, int status.
+ *
+ * Every entry point below replaces one function of r-ccs-cms/tnbp on the
+ * estimator hot path; the replaced interface is cited as path:line within
+ * that project.  The reference state is a set of caller-owned
+ * std::vector<TenT> (site tensors V, messages E/F); here the same state lives
+ * on the device inside a job handle and is mutated in place by these calls.
+ *
+ * Conventions shared with the reference (restated, not copied):
+ *  - Sites are the sorted distinct labels of the edge list
+ *    (GetSiteIndexFromBond, include/tnbp/framework/graph.h:23-35); a site is
+ *    addressed here by its position in that sorted list ("site index").
+ *  - Leg k of a site is the k-th edge, in edge-list order, that contains the
+ *    site (GetSurroundingBondIndex, graph.h:40-55); the physical leg is last.
+ *  - Tensors are column-major: coordinate 0 varies fastest.  Host buffers
+ *    are interleaved complex128 (re, im) unless stated otherwise.
+ *  - Messages: index m < n_edges is the message computed at edges[m].first
+ *    (absorbed by .second); index m + n_edges is the one computed at
+ *    edges[m].second (bp.h:170-174, 221-225).
+ *  - Status: 0 = success; a negative TNBP_E* code on failure, with a
+ *    readable message from tnbp_last_error() (per thread).  No call traps
+ *    the GPU to report an error.
+ */
+#ifndef TNBP_B200_H
+#define TNBP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define TNBP_OK 0
+#define TNBP_EINVAL -1      /* bad argument (std::invalid_argument in the reference) */
+#define TNBP_ECUDA -2       /* CUDA runtime error */
+#define TNBP_ENOMEM -3      /* device allocation failed / over the HBM budget */
+#define TNBP_ENOTCONV -4    /* bounded iteration limit reached (SVD sweeps) */
+#define TNBP_EPARSE -5      /* QASM / Pauli text parse error (qasm::ParseError, runtime_error) */
+#define TNBP_EUNSUPPORTED -6 /* gate or operator the reference also rejects */
+#define TNBP_ENOGPU -7      /* no CUDA device visible */
+
+/* ---- precision of a job's device state ---- */
+#define TNBP_C128 0 /* plain path: complex128 storage and arithmetic */
+#define TNBP_C64 1  /* mixed path: complex64 storage, FP32 products, FP64 sums
+                       and FP64 truncation eigensolves */
+
+typedef struct tnbp_job tnbp_job;
+typedef struct tnbp_tpo tnbp_tpo;
+
+/* Thread-local text of the last failure (empty string if none). */
+const char* tnbp_last_error(void);
+/* Library version string. */
+const char* tnbp_version(void);
+/* 1 if a CUDA device is visible, else 0.  Never fails. */
+int tnbp_device_available(void);
+
+/* ======================= host-side setup (bit-exact) ==================== */
+
+/* bond_square_lattice (include/tnbp/lattice/square.h:14-34).
+   Writes 2*(2*Lx*Ly-Lx-Ly) ints (pairs) to edges_out (capacity in pairs). */
+int tnbp_square_lattice(int32_t Lx, int32_t Ly, int32_t* edges_out, int64_t cap_pairs,
+                        int64_t* n_edges_out);
+
+/* GreedyEdgeLayering (graph.h:138-170): layer_of_edge[i] = layer of edge i. */
+int tnbp_greedy_layering(const int32_t* edges, int64_t n_edges, int32_t* layer_of_edge,
+                         int32_t* n_layers_out);
+
+/* GetSurroundingBondIndex (graph.h:40-55) for one site label. */
+int tnbp_surrounding_bonds(const int32_t* edges, int64_t n_edges, int32_t site_label,
+                           int32_t* bonds_out, int32_t cap, int32_t* n_out);
+
+/* FindShortestPath (graph.h:57-108): BFS path src..dst (labels). */
+int tnbp_shortest_path(const int32_t* edges, int64_t n_edges, int32_t src, int32_t dst,
+                       int32_t* path_out, int32_t cap, int32_t* n_out);
+
+/* qasm::parse_any (include/qasm/any.h:8-21) + EdgesFromQasm
+   (include/tnbp/parser/qasmtoedge.h:38-56).  Writes sorted unique
+   (min,max) pairs of the 2-qubit gates. */
+int tnbp_qasm_edges(const char* qasm_src, int32_t* edges_out, int64_t cap_pairs,
+                    int64_t* n_edges_out);
+
+/* qasm::parse_any: flattened instruction list.  For instruction i:
+   op[i] = qasm::Op enumerator value (include/qasm/ir.h:13-16),
+   nq[i] qubit indices in qubits[4*i..], np[i] params in params[3*i..].
+   Returns the count in n_out (call with cap 0 to size). */
+int tnbp_qasm_instructions(const char* qasm_src, int32_t* op, int32_t* nq, int32_t* qubits,
+                           int32_t* np, double* params, int64_t cap, int64_t* n_out);
+
+/* pauli::load_sparse_pauli_op (include/pauli/sparse_pauli.h:52-97) on text,
+   followed by SparsePauliToTensorOp + ClassifyOps
+   (include/tnbp/parser/paulitotpo.h:39-153).  For each kept term t:
+   kind[t] = 1 (one-site) or 2 (adjacent two-site); q0[t], q1[t] qubits
+   (ascending); letters[2t], letters[2t+1] = 'X','Y','Z'; coeff[2t..2t+1]
+   = (re, im); term_index[t] = its row in the file.  Terms the reference
+   drops (identity, >2 qubits, non-adjacent pairs) are counted in
+   n_dropped. */
+int tnbp_pauli_terms(const char* text, const int32_t* edges, int64_t n_edges, int32_t* kind,
+                     int32_t* q0, int32_t* q1, char* letters, double* coeff,
+                     int32_t* term_index, int64_t cap, int64_t* n_kept, int64_t* n_dropped);
+
+/* One TPO layer per barrier-delimited block of a QASM program
+   (QasmToTPO, include/tnbp/parser/qasmtotpo.h:743-767, built with
+   AppendGateToTPO 242-700 semantics).  Output for layer l:
+   edge_rank[l*n_edges + e] = TPO bond dim on edge e; op data packed per
+   site index in sorted-site order, each of shape (r_leg0..r_leg{g-1}, 2, 2)
+   column-major, complex128 interleaved.  op_offset[l*n_sites+s] is the
+   complex-element offset of site s in the packed buffer.  Call with
+   cap_elems 0 to size (n_layers_out, total elements in n_elems_out). */
+int tnbp_qasm_tpo(const char* qasm_src, const int32_t* edges, int64_t n_edges,
+                  int32_t* edge_rank, int64_t* op_offset, double* op_data, int64_t cap_elems,
+                  int32_t* n_layers_out, int64_t* n_elems_out);
+
+/* Kicked-Ising Floquet step as one TPO layer: exp(-i dt Jz ZZ) on every
+   edge in edge order, then exp(-i dt hz Z), then exp(-i dt hx X) on every
+   site (apps/kicked_ising_lattice/circuit.h:14-229).  The two-site gate is
+   split with the operator-Schmidt rank it has (2, or 1 when sin or cos of
+   dt*Jz vanishes); same output layout as tnbp_qasm_tpo with one layer. */
+int tnbp_kicked_ising_tpo(const int32_t* edges, int64_t n_edges, double Jz, double hz,
+                          double hx, double dt, int32_t* edge_rank, int64_t* op_offset,
+                          double* op_data, int64_t cap_elems, int64_t* n_elems_out);
+
+/* ============================ device state =============================== */
+
+/* InitTensorProductState (include/tnbp/ptns/function/init.h:18-95): product
+   state |0...0> (site tensors of shape (1,...,1,d) holding e_0), every
+   message the 1x1 tensor [1].  phys_dims may be NULL (all 2).  precision is
+   TNBP_C128 or TNBP_C64.  stream is a cudaStream_t (NULL = a stream the job
+   creates).  hbm_budget_bytes = 0 means no limit. */
+int tnbp_job_create(const int32_t* edges, int64_t n_edges, const int32_t* phys_dims,
+                    int32_t precision, void* stream, uint64_t hbm_budget_bytes, tnbp_job** out);
+int tnbp_job_destroy(tnbp_job* job);
+int tnbp_job_info(const tnbp_job* job, int64_t* n_sites, int64_t* n_edges, int32_t* precision);
+/* Bytes of device memory the job holds now. */
+int tnbp_job_device_bytes(const tnbp_job* job, uint64_t* bytes);
+/* Current bond dimension of every edge (n_edges ints). */
+int tnbp_bond_dims(const tnbp_job* job, int32_t* dims_out);
+
+/* Direct state access (the reference apps read/write std::vector<TenT>).
+   Shapes follow the conventions above; rank = degree + 1. */
+int tnbp_site_shape(const tnbp_job* job, int64_t site, int32_t* shape_out, int32_t cap,
+                    int32_t* rank_out);
+int tnbp_download_site(tnbp_job* job, int64_t site, double* data, int64_t cap_elems);
+int tnbp_upload_site(tnbp_job* job, int64_t site, const int32_t* shape, int32_t rank,
+                     const double* data);
+int tnbp_download_message(tnbp_job* job, int64_t m, double* data, int64_t cap_elems,
+                          int32_t* dim_out);
+/* Sets message m (dim x dim).  Both messages of an edge must end with the
+   edge's bond dimension before the next device call. */
+int tnbp_upload_message(tnbp_job* job, int64_t m, int32_t dim, const double* data);
+
+/* A TPO layer resident on the device (layout of tnbp_qasm_tpo, one layer). */
+int tnbp_tpo_create(tnbp_job* job, const int32_t* edge_rank, const int64_t* op_offset,
+                    const double* op_data, tnbp_tpo** out);
+int tnbp_tpo_destroy(tnbp_tpo* tpo);
+
+/* AbsorbTPO (include/tnbp/ptns/function/apply.h:15-177):
+   V'[(v_k,o_k)..., p'] = sum_p O[o..., p, p'] V[v..., p] with merged bond
+   index v + D*o, and every message E' = E (x) I_r. */
+int tnbp_absorb_tpo(tnbp_job* job, const tnbp_tpo* tpo);
+
+/* BeliefPropagation over all layers (bp.h:66-261) followed by the app's
+   F -> E copy (apps/estimator/main.cc:140-143): one Jacobi sweep. */
+int tnbp_bp_sweep(tnbp_job* job);
+
+/* BeliefPropagationCondition (bp.h:266-355) of the current messages:
+   mean over the 2|E| directed messages of
+   || normalize(recomputed) - normalize(stored) ||_F. */
+int tnbp_bp_condition(tnbp_job* job, double* result);
+
+/* The apps' BP loop (apps/estimator/main.cc:131-157): up to max_iter sweeps,
+   stop after the first whose condition is < tol.  Runs each sweep once
+   (the condition of sweep k is the distance between sweep k+1 and sweep
+   k, so the recomputation is shared).  iters_out = sweeps applied;
+   cond_out = last condition (NaN if max_iter == 0). */
+int tnbp_bp_run(tnbp_job* job, double tol, int32_t max_iter, int32_t* iters_out,
+                double* cond_out);
+
+/* Truncation (include/tnbp/ptns/function/truncation.h:18-222 with
+   SquareRootAndInverse, include/tnbp/framework/root.h:66-148): every edge
+   in parallel, FP64 on the device.  bond_dims_out / trunc_err_out hold
+   n_edges entries (may be NULL).  Rule for the kept singular values of
+   T = Ra^T Rb / ||.||: s_i > sv_min, at most chi_max, at least one;
+   trunc_err = discarded s^2 / total s^2. */
+int tnbp_truncate(tnbp_job* job, int32_t chi_max, double sv_min, int32_t* bond_dims_out,
+                  double* trunc_err_out);
+
+/* Measure, one-site (include/tnbp/ptns/function/measure.h:15-94):
+   out[2i..2i+1] = <O_i> at site index sites[i]; ops holds n 2x2 column-major
+   operators (ops[8i..8i+7]) in the reference's O[p, p'] layout. */
+int tnbp_measure_1site(tnbp_job* job, int64_t n, const int64_t* sites, const double* ops,
+                       double* out);
+
+/* Measure, nearest-neighbour two-site (measure.h:100-300): pairs[2i],
+   pairs[2i+1] are site LABELS (a, b) of an edge; ops holds n (2,2,2,2)
+   tensors O[p_a, p_b, p_a', p_b'] (ops[32i..32i+31]). */
+int tnbp_measure_2site(tnbp_job* job, int64_t n, const int32_t* pairs, const double* ops,
+                       double* out);
+
+/* Sum_k c_k <P_k> in FP64 on the device over kept Pauli terms
+   (same layout as tnbp_pauli_terms).  Not in the reference (which prints
+   per-term values, apps/estimator/main.cc:213-238); per-term values are
+   written to per_term_out (2 doubles each, may be NULL). */
+int tnbp_measure_pauli_sum(tnbp_job* job, int64_t n_terms, const int32_t* kind,
+                           const int32_t* q0, const int32_t* q1, const char* letters,
+                           const double* coeff, double* per_term_out, double* sum_out);
+
+/* Time spent in the job's last bp sweep kernels (ms, CUDA events) and the
+   algorithmic flops/bytes of one sweep at the current shapes. */
+int tnbp_sweep_stats(const tnbp_job* job, double* last_sweep_ms, double* flops,
+                     double* bytes);
+
+/* ============================ served path =============================== */
+
+typedef struct tnbp_server tnbp_server;
+
+/* Continuous-batching request loop on one GPU: jobs are admitted while
+   their HBM footprint fits hbm_budget_bytes and max_active slots are free;
+   BP sweeps of all active jobs run as one batched launch per stage. */
+int tnbp_server_create(int32_t precision, uint64_t hbm_budget_bytes, int32_t max_active,
+                       tnbp_server** out);
+int tnbp_server_destroy(tnbp_server* srv);
+/* Kicked-Ising estimator request on an L x L open square lattice:
+   n_steps Floquet steps of RZZ(theta_j) on all edges then RX(theta_h) on all
+   sites, BP(tol, max_iter), truncation to chi, then sum_k c_k <P_k>. */
+int tnbp_server_submit_kicked_ising(tnbp_server* srv, int32_t L, int32_t chi, int32_t n_steps,
+                                    double theta_j, double theta_h, double bp_tol,
+                                    int32_t bp_max_iter, double sv_min, int64_t n_terms,
+                                    const int32_t* kind, const int32_t* q0, const int32_t* q1,
+                                    const char* letters, const double* coeff,
+                                    int64_t* request_id);
+/* Advance the loop once (admission + one batched stage).  n_done_out =
+   number of requests that completed during this call. */
+int tnbp_server_step(tnbp_server* srv, int32_t* n_active_out, int32_t* n_queued_out,
+                     int32_t* n_done_out);
+/* Result of a finished request: sum (re, im), 0 if done, 1 if pending. */
+int tnbp_server_result(tnbp_server* srv, int64_t request_id, double* sum_out,
+                       int32_t* pending_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,276 @@
+"""Regenerate the golden fixtures in tests/golden/ from the reference itself.
+
+The fixtures pin the oracle and the B200 engine to r-ccs-cms/tnbp's own code:
+the reference's unchanged headers and apps are compiled by oracle/Makefile
+(against the project's CPU gqten and single-rank MPI stand-ins) into
+oracle/_ref/, and this script runs them on seeded synthetic inputs:
+
+  probe_<name>.npz   every intermediate tensor of the estimator loop
+                     (oracle/ref_probe.cc): TPO layers, V/E after AbsorbTPO,
+                     E after the first BP sweep and after BP, conditions,
+                     truncation dims/errors, V/E after truncation, one- and
+                     two-site expectation values
+  host_<name>.json   lattice edges, greedy layers, leg order, BFS paths,
+                     parsed QASM instructions, TPO layer shapes, Pauli
+                     classification (oracle/ref_hostparity.cc)
+  config1.json       observables of the 4x4 kicked-Ising workload from the
+                     reference apps kicked_ising_lattice and estimator
+
+usage: python tests/golden/make_golden.py [--ref /root/reference]
+Needs the reference sources (only in the build container); the fixtures it
+writes are what the tests read everywhere else.
+"""
+import argparse
+import json
+import math
+import os
+import re
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, HERE)
+from records import read_records  # noqa: E402
+
+INPUTS = os.path.join(HERE, "inputs")
+REF_BIN = os.path.join(ROOT, "oracle", "_ref")
+
+
+# ----------------------------------------------------------- input writers
+def lattice_edges(L):
+    e = []
+    for iy in range(L):
+        for ix in range(L):
+            s = ix + L * iy
+            if ix + 1 < L:
+                e.append((s, s + 1))
+            if iy + 1 < L:
+                e.append((s, s + L))
+    return e
+
+
+def kicked_ising_qasm(Lx, Ly, steps, theta_j, theta_h):
+    """RZZ(theta_j) on horizontal then vertical edges, RX(theta_h) on every
+    site, one barrier per step (the 4x4 kicked-Ising workload's form)."""
+    n = Lx * Ly
+    out = ["OPENQASM 2.0;", 'include "qelib1.inc";', f"qreg q[{n}];"]
+    for _ in range(steps):
+        for iy in range(Ly):
+            for ix in range(Lx - 1):
+                i = ix + Lx * iy
+                out.append(f"rzz({theta_j!r}) q[{i}],q[{i + 1}];")
+        for iy in range(Ly - 1):
+            for ix in range(Lx):
+                i = ix + Lx * iy
+                out.append(f"rzz({theta_j!r}) q[{i}],q[{i + Lx}];")
+        for i in range(n):
+            out.append(f"rx({theta_h!r}) q[{i}];")
+        out.append("barrier q;")
+    return "\n".join(out) + "\n"
+
+
+def colourings(Lx, Ly):
+    hev = [(ix + Lx * iy, ix + 1 + Lx * iy) for iy in range(Ly) for ix in range(0, Lx - 1, 2)]
+    hod = [(ix + Lx * iy, ix + 1 + Lx * iy) for iy in range(Ly) for ix in range(1, Lx - 1, 2)]
+    vev = [(ix + Lx * iy, ix + Lx * (iy + 1)) for iy in range(0, Ly - 1, 2) for ix in range(Lx)]
+    vod = [(ix + Lx * iy, ix + Lx * (iy + 1)) for iy in range(1, Ly - 1, 2) for ix in range(Lx)]
+    return [hev, hod, vev, vod]
+
+
+def random_circuit_qasm(Lx, Ly, layers, rng):
+    """U3(theta, phi, lambda ~ U[0, 2pi)) on every qubit, then CZ on edge
+    colouring (layer mod 4): H-even, H-odd, V-even, V-odd."""
+    n = Lx * Ly
+    out = ["OPENQASM 2.0;", 'include "qelib1.inc";', f"qreg q[{n}];"]
+    # every lattice edge appears once in a leading identity-free CZ^2 pass so
+    # the edge list (EdgesFromQasm) is the full lattice
+    cols = colourings(Lx, Ly)
+    for layer in range(layers):
+        for i in range(n):
+            a, b, c = (float(v) for v in rng.uniform(0, 2 * math.pi, 3))
+            out.append(f"u3({a!r},{b!r},{c!r}) q[{i}];")
+        for (i, j) in cols[layer % 4]:
+            out.append(f"cz q[{i}],q[{j}];")
+        out.append("barrier q;")
+    return "\n".join(out) + "\n"
+
+
+def random_paulis(n, edges, nterms, rng, extra_text=True):
+    lines = ["# seeded sparse Pauli observable", "// second comment style", ""]
+    letters = "XYZ"
+    for t in range(nterms):
+        k = int(rng.integers(1, 5))
+        if t % 5 == 0:
+            a, b = edges[int(rng.integers(0, len(edges)))]
+            qs = [a, b]
+        else:
+            qs = list(rng.choice(n, size=min(k, n), replace=False))
+        s = ["I"] * n
+        for q in qs:
+            s[n - 1 - int(q)] = letters[int(rng.integers(0, 3))]
+        c = float(rng.normal())
+        if t % 3 == 0:
+            lines.append(f"{c!r} {float(rng.normal())!r} {''.join(s)}")
+        else:
+            lines.append(f"{c!r} {''.join(s).lower() if t % 7 == 0 else ''.join(s)}")
+    lines.append(f"0.5 {'I' * n}")  # identity term: dropped by ClassifyOps
+    return "\n".join(lines) + "\n"
+
+
+# ------------------------------------------------------------------ runners
+def run_probe(name, qasm, pauli, chi, sv_min, tol, maxit, lattice=None):
+    qp = os.path.join(INPUTS, f"{name}.qasm")
+    pp = os.path.join(INPUTS, f"{name}.txt")
+    with open(qp, "w") as f:
+        f.write(qasm)
+    with open(pp, "w") as f:
+        f.write(pauli)
+    out = os.path.join("/tmp", f"probe_{name}.bin")
+    extra = [str(lattice[0]), str(lattice[1])] if lattice else []
+    subprocess.check_call([os.path.join(REF_BIN, "ref_probe"), qp, pp, out, str(chi), repr(sv_min),
+                           repr(tol), str(maxit)] + extra)
+    recs = read_records(out)
+    meta = dict(chi=chi, sv_min=sv_min, tol=tol, maxit=maxit, lattice=lattice)
+    np.savez_compressed(os.path.join(HERE, f"probe_{name}.npz"), __meta__=json.dumps(meta), **recs)
+    print(f"probe_{name}: {len(recs)} records")
+
+
+def run_hostparity(name, args):
+    out = subprocess.check_output([os.path.join(REF_BIN, "ref_hostparity")] + args, text=True)
+    data = json.loads(out)
+    with open(os.path.join(HERE, f"host_{name}.json"), "w") as f:
+        json.dump(data, f, separators=(",", ":"))
+    print(f"host_{name}: keys {sorted(data)}")
+
+
+def run_config1():
+    """4x4 open lattice, 5 steps of RZZ(-pi/2) on every edge then RX(0.8),
+    chi = 4, BP tolerance 1e-10, at most 50 sweeps; <Z> on site 5 = (1,1).
+    kicked_ising_lattice flags: dt*Jz = theta_J/2 with dt = 0.25 (x pi),
+    Jz = -1; dt*hx = 0.4 -> hx = 1.6/pi."""
+    res = {}
+    hx = 1.6 / math.pi
+    out = subprocess.check_output(
+        [os.path.join(REF_BIN, "kicked_ising_lattice"), "--lattice", "square", "--L", "4", "--dt", "0.25",
+         "--Jz", "-1", "--hz", "0", "--hx", repr(hx), "--num_steps", "5", "--max_bond_dim", "4",
+         "--bp_tolerance", "1e-10", "--max_bp_iterations", "50"], text=True)
+    z = {}
+    x = {}
+    zz = {}
+    conds = []
+    for line in out.splitlines():
+        m = re.search(r"measurement of Z at site (\d+) time step (\d+) = (\S+)", line)
+        if m:
+            z[f"{m.group(2)}/{m.group(1)}"] = float(m.group(3))
+        m = re.search(r"measurement of X at site (\d+) time step (\d+) = (\S+)", line)
+        if m:
+            x[f"{m.group(2)}/{m.group(1)}"] = float(m.group(3))
+        m = re.search(r"measurement of ZZ at sites \((\d+),(\d+)\) time step (\d+) = (\S+)", line)
+        if m:
+            zz[f"{m.group(3)}/{m.group(1)},{m.group(2)}"] = float(m.group(4))
+        m = re.search(r"condition at time step (\d+) = (\S+)", line)
+        if m:
+            conds.append([int(m.group(1)), float(m.group(2))])
+    res["kicked_ising_lattice"] = dict(Z=z, X=x, ZZ=zz, conditions=conds, hx=hx)
+    qasm = kicked_ising_qasm(4, 4, 5, -math.pi / 2, 0.8)
+    qp = os.path.join(INPUTS, "config1.qasm")
+    pp = os.path.join(INPUTS, "config1.txt")
+    with open(qp, "w") as f:
+        f.write(qasm)
+    with open(pp, "w") as f:
+        f.write("1.0 0.0 " + "".join("Z" if 15 - k == 5 else "I" for k in range(16)) + "\n")
+    out = subprocess.check_output(
+        [os.path.join(REF_BIN, "estimator"), "--circuit", qp, "--sparse_pauli", pp, "--max_bond_dim", "4",
+         "--bp_tolerance", "1e-10", "--max_bp_iterations", "50", "--sv_min", "1e-8"], text=True)
+    m = re.search(r"single site operator at site 5 (\S+)", out)
+    dims = [int(v) for v in re.findall(r"bond dim = (\d+)", out)]
+    errs = [float(v) for v in re.findall(r"truncation error for edge \(\d+,\d+\) = (\S+)", out)]
+    conds = [float(v) for v in re.findall(r"condition at step \d+ = (\S+)", out)]
+    res["estimator"] = dict(Z5=float(m.group(1)), bond_dims=dims, trunc_errs=errs, conditions=conds)
+    with open(os.path.join(HERE, "config1.json"), "w") as f:
+        json.dump(res, f, indent=1)
+    print("config1:", res["estimator"]["Z5"], res["kicked_ising_lattice"]["Z"].get("4/5"))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", default="")
+    a = ap.parse_args()
+    subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), f"REF={a.ref}"])
+    os.makedirs(INPUTS, exist_ok=True)
+    rng = np.random.default_rng(20261203)
+    jobs = a.only.split(",") if a.only else ["probe", "host", "config1"]
+    if "probe" in jobs:
+        # P1: 3x3 kicked Ising, 3 steps, chi 2 (BP at D <= 4)
+        q = kicked_ising_qasm(3, 3, 3, -math.pi / 2, 0.8)
+        run_probe("ki3x3", q, random_paulis(9, lattice_edges(3), 12, rng), 2, 1e-8, 1e-10, 30)
+        # P2: 3x3 random circuit, 4 layers, chi 4
+        q = random_circuit_qasm(3, 3, 4, rng)
+        # the colourings of 4 layers cover every edge, so EdgesFromQasm = lattice
+        run_probe("rc3x3", q, random_paulis(9, lattice_edges(3), 16, rng), 4, 1e-8, 1e-10, 30)
+        # P3: open chain of 6 (a tree: BP is exact), random circuit, no truncation
+        chain = [(i, i + 1) for i in range(5)]
+        lines = ["OPENQASM 2.0;", 'include "qelib1.inc";', "qreg q[6];"]
+        for layer in range(3):
+            for i in range(6):
+                a_, b_, c_ = (float(v) for v in rng.uniform(0, 2 * math.pi, 3))
+                lines.append(f"u3({a_!r},{b_!r},{c_!r}) q[{i}];")
+            for i in range(layer % 2, 5, 2):
+                lines.append(f"cx q[{i}],q[{i + 1}];")
+            lines.append("barrier q;")
+        run_probe("chain6", "\n".join(lines) + "\n", random_paulis(6, chain, 10, rng), 64, 1e-12, 1e-13, 40)
+        # P4: 2x3 lattice with a distance-2 gate (identity pass-through tensor)
+        lines = ["OPENQASM 2.0;", 'include "qelib1.inc";', "qreg q[6];"]
+        for (i, j) in lattice_edges_rect(3, 2):
+            lines.append(f"cz q[{i}],q[{j}];")
+        lines.append("barrier q;")
+        for i in range(6):
+            lines.append(f"h q[{i}];")
+        lines.append("cx q[0],q[2];")
+        lines.append("rzz(0.37) q[3],q[5];")
+        lines.append("barrier q;")
+        lines.append("ry(0.3) q[1];")
+        lines.append("barrier q;")
+        run_probe("pass2x3", "\n".join(lines) + "\n", random_paulis(6, lattice_edges_rect(3, 2), 10, rng), 8,
+                  1e-10, 1e-12, 40, lattice=(3, 2))
+    if "host" in jobs:
+        run_hostparity("lattice4x4", ["lattice", "4", "4"])
+        run_hostparity("lattice16x16", ["lattice", "16", "16"])
+        run_hostparity("lattice5x3", ["lattice", "5", "3"])
+        for nm in ["ki3x3", "rc3x3", "chain6"]:
+            run_hostparity(nm, ["qasm", os.path.join(INPUTS, f"{nm}.qasm"), os.path.join(INPUTS, f"{nm}.txt")])
+        run_hostparity("pass2x3", ["qasm", os.path.join(INPUTS, "pass2x3.qasm"),
+                                   os.path.join(INPUTS, "pass2x3.txt"), "3", "2"])
+        kob = os.path.join(a.ref, "apps", "estimator")
+        run_hostparity("kobe", ["qasm", os.path.join(kob, "kicked_ising.qasm"), os.path.join(kob, "H_ising_kobe.txt")])
+        run_hostparity("ising_circuit", ["qasm", os.path.join(a.ref, "apps", "qasm_tpo", "ising_circuit.qasm")])
+        # a v3-syntax program exercising slices, bit declarations and measure assignments
+        v3 = ("OPENQASM 3;\ninclude \"stdgates.inc\";\nqubit[5] q;\nbit[2] c;\n"
+              "h q[0:3];\ncx q[0], q[1];\nrz(-pi/4 + 2*0.1) q[2];\nrzz(tau/8) q[2],q[3];\n"
+              "/* block */ cz q[3],q[4]; // tail\nbarrier q;\nu(1e-1, .5, -2.5e0) q[4];\n"
+              "c[0] = measure q[0];\nbit x = measure q[1];\n")
+        with open(os.path.join(INPUTS, "v3.qasm"), "w") as f:
+            f.write(v3)
+        run_hostparity("v3", ["qasm", os.path.join(INPUTS, "v3.qasm")])
+    if "config1" in jobs:
+        run_config1()
+
+
+def lattice_edges_rect(Lx, Ly):
+    e = []
+    for iy in range(Ly):
+        for ix in range(Lx):
+            s = ix + Lx * iy
+            if ix + 1 < Lx:
+                e.append((s, s + 1))
+            if iy + 1 < Ly:
+                e.append((s, s + Lx))
+    return e
+
+
+if __name__ == "__main__":
+    main()

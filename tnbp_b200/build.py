@@ -1,0 +1,71 @@
+"""Build libtnbp_b200.so in-tree for sm_100a with nvcc.
+
+Usage: python -m tnbp_b200.build  (or tnbp_b200.build.build()).
+Objects are cached under tnbp_b200/_build/ and rebuilt when a source or
+header is newer than its object.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libtnbp_b200.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+SOURCES = ["engine.cu", "capi.cu", "server.cu", "host_setup.cpp"]
+
+
+def _headers():
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    hs.append(os.path.join(INCLUDE, "tnbp_b200.h"))
+    return hs
+
+
+def _stale(obj, src):
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(p) > t for p in [src] + _headers())
+
+
+def build(verbose=True, jobs=4):
+    os.makedirs(BUILD, exist_ok=True)
+    objs, procs = [], []
+    for s in SOURCES:
+        src = os.path.join(CSRC, s)
+        if not os.path.exists(src):
+            continue
+        obj = os.path.join(BUILD, s + ".o")
+        objs.append(obj)
+        if not _stale(obj, src):
+            continue
+        if s.endswith(".cu"):
+            cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+                   "--expt-relaxed-constexpr", "-c", src, "-o", obj]
+        else:
+            cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append((subprocess.Popen(cmd), cmd))
+        if len(procs) >= jobs:
+            p, c = procs.pop(0)
+            if p.wait() != 0:
+                raise RuntimeError("compile failed: " + " ".join(c))
+    for p, c in procs:
+        if p.wait() != 0:
+            raise RuntimeError("compile failed: " + " ".join(c))
+    if not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
+        cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", LIB, "-lcudart_static",
+               "-lrt", "-lpthread", "-ldl"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
+    return LIB
+
+
+if __name__ == "__main__":
+    build()
+    sys.exit(0)

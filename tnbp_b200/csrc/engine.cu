@@ -1,0 +1,1002 @@
+// Device-resident BP-PEPS estimator engine behind the C ABI of
+// include/tnbp_b200.h.  One job = one PEPS (site tensors V, two message
+// arenas E/F) on one GPU stream.  Host code only builds task descriptors;
+// all tensor arithmetic runs in the kernels of kernels.cuh, truncate.cuh and
+// measure.cuh.  There is no CPU fallback: without a device every state call
+// fails with TNBP_ENOGPU.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tnbp_b200.h"
+#include "engine.h"
+#include "kernels.cuh"
+#include "measure.cuh"
+#include "truncate.cuh"
+
+namespace tnbp {
+
+thread_local std::string g_last_error;
+
+void check_cuda(cudaError_t e, const char* what, const char* file, int line) {
+  if (e != cudaSuccess) {
+    throw Error(TNBP_ECUDA, std::string(what) + ": " + cudaGetErrorString(e) + " (" + file + ":" +
+                                std::to_string(line) + ")");
+  }
+}
+
+// ----------------------------------------------------------------- memory
+DevBuf::~DevBuf() { release(); }
+void DevBuf::release() {
+  if (p) {
+    cudaFreeAsync(p, stream);
+    p = nullptr;
+  }
+  bytes = 0;
+}
+void DevBuf::alloc(size_t nbytes, cudaStream_t s) {
+  release();
+  stream = s;
+  if (nbytes == 0) return;
+  cudaError_t e = cudaMallocAsync(&p, nbytes, s);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    cudaGetLastError();
+    throw Error(TNBP_ENOMEM, "device allocation of " + std::to_string(nbytes) + " bytes failed: " +
+                                 cudaGetErrorString(e));
+  }
+  bytes = nbytes;
+}
+
+template <typename T>
+static void upload_vec(DevBuf& b, const std::vector<T>& v, cudaStream_t s) {
+  b.alloc(std::max<size_t>(sizeof(T), v.size() * sizeof(T)), s);
+  if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+static inline size_t align_elems(size_t n) { return (n + 31) & ~size_t(31); }
+
+// ------------------------------------------------------------------ graph
+Graph::Graph(const int32_t* e, int64_t n) {
+  if (n <= 0 || !e) throw Error(TNBP_EINVAL, "edge list is empty");
+  edges.resize(n);
+  for (int64_t i = 0; i < n; ++i) {
+    edges[i] = {e[2 * i], e[2 * i + 1]};
+    if (edges[i].first == edges[i].second) throw Error(TNBP_EINVAL, "self-loop edge");
+  }
+  // GetSiteIndexFromBond (graph.h:23-35): sorted distinct labels
+  for (auto& p : edges) { labels.push_back(p.first); labels.push_back(p.second); }
+  std::sort(labels.begin(), labels.end());
+  labels.erase(std::unique(labels.begin(), labels.end()), labels.end());
+  for (size_t s = 0; s < labels.size(); ++s) index_of[labels[s]] = (int)s;
+  // GetSurroundingBondIndex (graph.h:40-55): incident edges in edge order
+  legs.assign(labels.size(), {});
+  leg_a.resize(n);
+  leg_b.resize(n);
+  site_a.resize(n);
+  site_b.resize(n);
+  for (int64_t m = 0; m < n; ++m) {
+    const int a = index_of[edges[m].first], b = index_of[edges[m].second];
+    site_a[m] = a;
+    site_b[m] = b;
+    leg_a[m] = (int)legs[a].size();
+    legs[a].push_back((int)m);
+    leg_b[m] = (int)legs[b].size();
+    legs[b].push_back((int)m);
+  }
+  for (auto& l : legs)
+    if ((int)l.size() > kMaxLegs) throw Error(TNBP_EINVAL, "site degree above " + std::to_string(kMaxLegs));
+}
+
+// message index computed at site s along its leg k, and the one it absorbs
+int Graph::out_msg(int s, int k) const {
+  const int e = legs[s][k];
+  return site_a[e] == s ? e : e + (int)edges.size();
+}
+int Graph::in_msg(int s, int k) const {
+  const int e = legs[s][k];
+  return site_a[e] == s ? e + (int)edges.size() : e;
+}
+
+// -------------------------------------------------------------------- job
+Job::Job(const int32_t* e, int64_t n, const int32_t* pdims, int precision, cudaStream_t s,
+         uint64_t budget)
+    : g(e, n), prec(precision), budget(budget) {
+  if (precision != TNBP_C128 && precision != TNBP_C64) throw Error(TNBP_EINVAL, "unknown precision");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    throw Error(TNBP_ENOGPU, "no CUDA device visible: the B200 engine has no CPU path");
+  }
+  esz = prec == TNBP_C128 ? 16 : 8;
+  if (s) {
+    stream = s;
+  } else {
+    CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    own_stream = true;
+  }
+  CK(cudaEventCreate(&ev0));
+  CK(cudaEventCreate(&ev1));
+  CK(cudaMallocHost(&host_scalar, 64));
+  const int ns = (int)g.labels.size();
+  pd.assign(ns, 2);
+  if (pdims) for (int i = 0; i < ns; ++i) pd[i] = pdims[i];
+  dim.assign(g.edges.size(), 1);
+  layout();
+  V.alloc(v_elems * esz, stream);
+  M[0].alloc(m_elems * esz, stream);
+  M[1].alloc(m_elems * esz, stream);
+  // |0...0>: V_s = e_0 on the physical leg; messages = [1] (init.h:40-61)
+  std::vector<double> hv(2 * v_elems, 0.0), hm(2 * m_elems, 0.0);
+  for (int s = 0; s < ns; ++s) hv[2 * voff[s]] = 1.0;
+  for (size_t m = 0; m < moff.size(); ++m) hm[2 * moff[m]] = 1.0;
+  put_complex(V, hv.data(), v_elems, 0);
+  put_complex(M[0], hm.data(), m_elems, 0);
+  cur = 0;
+  CK(cudaStreamSynchronize(stream));
+  check_budget();
+}
+
+Job::~Job() {
+  destroy_graphs();
+  cudaStreamSynchronize(stream);
+  V.release(); M[0].release(); M[1].release();
+  plan = SweepPlan();
+  if (host_scalar) cudaFreeHost(host_scalar);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  cudaStreamSynchronize(stream);
+  if (own_stream) cudaStreamDestroy(stream);
+}
+
+std::vector<int> Job::site_shape(int s) const {
+  std::vector<int> sh;
+  for (int e : g.legs[s]) sh.push_back(dim[e]);
+  sh.push_back(pd[s]);
+  return sh;
+}
+size_t Job::site_elems(int s) const {
+  size_t n = pd[s];
+  for (int e : g.legs[s]) n *= dim[e];
+  return n;
+}
+
+void Job::layout() {
+  const int ns = (int)g.labels.size();
+  const int ne = (int)g.edges.size();
+  voff.assign(ns, 0);
+  size_t o = 0;
+  for (int s = 0; s < ns; ++s) { voff[s] = o; o += align_elems(site_elems(s)); }
+  v_elems = std::max<size_t>(o, 32);
+  moff.assign(2 * ne, 0);
+  o = 0;
+  for (int m = 0; m < 2 * ne; ++m) {
+    const size_t dd = (size_t)dim[m % ne] * dim[m % ne];
+    moff[m] = o;
+    o += align_elems(dd);
+  }
+  m_elems = std::max<size_t>(o, 32);
+}
+
+void Job::put_complex(DevBuf& dst, const double* src, size_t n, size_t elem_off) {
+  if (n == 0) return;
+  if (prec == TNBP_C128) {
+    CK(cudaMemcpyAsync(static_cast<char*>(dst.p) + elem_off * 16, src, n * 16, cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+  } else {
+    std::vector<float> f(2 * n);
+    for (size_t i = 0; i < 2 * n; ++i) f[i] = (float)src[i];
+    CK(cudaMemcpyAsync(static_cast<char*>(dst.p) + elem_off * 8, f.data(), n * 8, cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+}
+void Job::get_complex(const DevBuf& src, double* dst, size_t n, size_t elem_off) {
+  if (n == 0) return;
+  if (prec == TNBP_C128) {
+    CK(cudaMemcpyAsync(dst, static_cast<const char*>(src.p) + elem_off * 16, n * 16, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+  } else {
+    std::vector<float> f(2 * n);
+    CK(cudaMemcpyAsync(f.data(), static_cast<const char*>(src.p) + elem_off * 8, n * 8, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    for (size_t i = 0; i < 2 * n; ++i) dst[i] = f[i];
+  }
+}
+
+uint64_t Job::device_bytes() const {
+  return V.bytes + M[0].bytes + M[1].bytes + plan.bytes();
+}
+void Job::check_budget() const {
+  if (budget && device_bytes() > budget)
+    throw Error(TNBP_ENOMEM, "job needs " + std::to_string(device_bytes()) + " device bytes, budget " +
+                                 std::to_string(budget));
+}
+
+void* Job::vptr(int s) const { return static_cast<char*>(V.p) + voff[s] * esz; }
+void* Job::mptr(int arena, int m) const { return static_cast<char*>(M[arena].p) + moff[m] * esz; }
+
+void Job::destroy_graphs() {
+  for (int i = 0; i < 2; ++i) {
+    if (plan.graph_exec[i]) { cudaGraphExecDestroy(plan.graph_exec[i]); plan.graph_exec[i] = nullptr; }
+  }
+}
+
+SweepPlan::~SweepPlan() {}
+uint64_t SweepPlan::bytes() const {
+  uint64_t b = scratch.bytes + partial.bytes + dist.bytes + cond.bytes + gram_tasks.bytes +
+               gram_begins.bytes + msg_tasks[0].bytes + msg_tasks[1].bytes;
+  for (auto& l : levels) b += l.tasks[0].bytes + l.tasks[1].bytes + l.begins.bytes;
+  return b;
+}
+
+// --------------------------------------------------------------- sweep plan
+// Messages T_t = V x_{k != t} E_k for all targets t of a site share partial
+// products: targets are split in halves, the legs of the other half are
+// absorbed once for each half, and the recursion continues.  A degree-4
+// site needs 8 leg contractions instead of the 12 of the leg-by-leg
+// schedule of bp.h:137-154 (the same products in another association; the
+// per-leg normalizations of bp.h:153 only rescale, and the final
+// normalization of bp.h:166 removes the scale).
+namespace {
+struct PlanOp { int site, src, dst, leg, level; };
+struct SitePlanner {
+  int site;
+  std::vector<PlanOp>* ops;
+  int next_slot = 0;
+  std::vector<int> result;  // slot holding T_t (-1 = V itself)
+  int chain(int src, int level, const std::vector<int>& legs, int* out_level) {
+    int cur = src, lv = level;
+    for (int leg : legs) {
+      const int dst = next_slot++;
+      ops->push_back({site, cur, dst, leg, lv});
+      cur = dst;
+      ++lv;
+    }
+    *out_level = lv;
+    return cur;
+  }
+  void rec(int src, int level, const std::vector<int>& targets, std::vector<char> absorbed, int g) {
+    if (targets.size() == 1) {
+      std::vector<int> rest;
+      for (int k = 0; k < g; ++k) if (k != targets[0] && !absorbed[k]) rest.push_back(k);
+      int lv;
+      result[targets[0]] = chain(src, level, rest, &lv);
+      return;
+    }
+    const size_t h = targets.size() / 2;
+    std::vector<int> h1(targets.begin(), targets.begin() + h), h2(targets.begin() + h, targets.end());
+    for (int part = 0; part < 2; ++part) {
+      const auto& keep = part == 0 ? h1 : h2;
+      const auto& other = part == 0 ? h2 : h1;
+      std::vector<int> legs;
+      for (int k : other) if (!absorbed[k]) legs.push_back(k);
+      int lv;
+      const int x = chain(src, level, legs, &lv);
+      auto ab = absorbed;
+      for (int k : legs) ab[k] = 1;
+      rec(x, lv, keep, ab, g);
+    }
+  }
+};
+}  // namespace
+
+void Job::build_plan() {
+  destroy_graphs();
+  plan = SweepPlan();
+  const int ns = (int)g.labels.size();
+  const int ne = (int)g.edges.size();
+  std::vector<PlanOp> ops;
+  std::vector<std::vector<int>> result(ns);
+  std::vector<int> nslots(ns, 0);
+  for (int s = 0; s < ns; ++s) {
+    const int gs = (int)g.legs[s].size();
+    SitePlanner sp;
+    sp.site = s;
+    sp.ops = &ops;
+    sp.result.assign(gs, -1);
+    std::vector<int> targets(gs);
+    std::iota(targets.begin(), targets.end(), 0);
+    sp.rec(-1, 0, targets, std::vector<char>(gs, 0), gs);
+    result[s] = sp.result;
+    nslots[s] = sp.next_slot;
+  }
+  // scratch: every slot of a site holds one site-sized tensor
+  std::vector<size_t> slot_base(ns, 0);
+  size_t o = 0;
+  for (int s = 0; s < ns; ++s) { slot_base[s] = o; o += (size_t)nslots[s] * align_elems(site_elems(s)); }
+  plan.scratch.alloc(std::max<size_t>(o, 32) * esz, stream);
+  auto slot_ptr = [&](int s, int slot) -> void* {
+    if (slot < 0) return vptr(s);
+    return static_cast<char*>(plan.scratch.p) + (slot_base[s] + (size_t)slot * align_elems(site_elems(s))) * esz;
+  };
+  int maxlevel = 0;
+  for (auto& op : ops) maxlevel = std::max(maxlevel, op.level + 1);
+  plan.levels.resize(maxlevel);
+  plan.flops = 0.0;
+  plan.bytes_alg = 0.0;
+  for (int lv = 0; lv < maxlevel; ++lv) {
+    std::vector<LegTask> t[2];
+    std::vector<long long> begins;
+    long long nb = 0;
+    int maxdin = 1;
+    for (auto& op : ops) {
+      if (op.level != lv) continue;
+      const auto sh = site_shape(op.site);
+      long long L = 1, R = 1;
+      for (int k = 0; k < op.leg; ++k) L *= sh[k];
+      for (size_t k = op.leg + 1; k < sh.size(); ++k) R *= sh[k];
+      const int D = sh[op.leg];
+      for (int par = 0; par < 2; ++par) {
+        LegTask lt;
+        lt.in = slot_ptr(op.site, op.src);
+        lt.out = slot_ptr(op.site, op.dst);
+        lt.mat = mptr(par, g.in_msg(op.site, op.leg));
+        lt.L = L; lt.R = R; lt.Din = D; lt.Dout = D;
+        lt.block_begin = nb;
+        t[par].push_back(lt);
+      }
+      begins.push_back(nb);
+      nb += (L * R + kRowTile - 1) / kRowTile;
+      maxdin = std::max(maxdin, D);
+    }
+    upload_vec(plan.levels[lv].tasks[0], t[0], stream);
+    upload_vec(plan.levels[lv].tasks[1], t[1], stream);
+    upload_vec(plan.levels[lv].begins, begins, stream);
+    plan.levels[lv].ntask = (int)t[0].size();
+    plan.levels[lv].nblocks = nb;
+    plan.levels[lv].max_din = maxdin;
+  }
+  // Gram + finalize tasks, one per directed message
+  std::vector<GramTask> gt;
+  std::vector<long long> gbeg;
+  std::vector<MsgTask> mt[2];
+  long long nb = 0;
+  size_t part_elems = 0;
+  struct Pending { int s, t; size_t part_off; int nchunk, C; };
+  std::vector<Pending> pend;
+  for (int s = 0; s < ns; ++s) {
+    const auto sh = site_shape(s);
+    const int gs = (int)g.legs[s].size();
+    const double n = (double)site_elems(s);
+    double sumD = 0;
+    for (int k = 0; k < gs; ++k) sumD += sh[k];
+    // algorithmic work of bp.h's schedule: 8 d prod(D) sum(D) flops per message
+    plan.flops += gs * 8.0 * n * sumD;
+    plan.bytes_alg += n * esz + 2.0 * gs * 0.0;
+    for (int t = 0; t < gs; ++t) {
+      GramTask g1;
+      g1.A = slot_ptr(s, result[s][t]);
+      g1.B = vptr(s);
+      long long L = 1, M = 1;
+      for (int k = 0; k < t; ++k) L *= sh[k];
+      for (size_t k = t + 1; k < sh.size(); ++k) M *= sh[k];
+      g1.L = L; g1.M = M; g1.D = sh[t]; g1.P = 1; g1.C = sh[t];
+      g1.ctiles = (g1.C + kColTile - 1) / kColTile;
+      g1.Q = L * M;
+      long long cr = ((g1.Q / 16) + kRowTile - 1) / kRowTile * kRowTile;
+      cr = std::max<long long>(256, std::min<long long>(4096, cr));
+      g1.chunk_rows = cr;
+      g1.nchunk = (int)((g1.Q + cr - 1) / cr);
+      g1.partial = nullptr;
+      g1.block_begin = nb;
+      gbeg.push_back(nb);
+      nb += (long long)g1.nchunk * g1.ctiles * g1.ctiles;
+      pend.push_back({s, t, part_elems, g1.nchunk, g1.C});
+      part_elems += (size_t)g1.nchunk * g1.C * g1.C;
+      gt.push_back(g1);
+      plan.bytes_alg += 2.0 * sh[t] * sh[t] * esz;  // message in + out
+    }
+  }
+  plan.partial.alloc(std::max<size_t>(part_elems, 1) * sizeof(double2), stream);
+  plan.dist.alloc(std::max<size_t>(2 * ne, 1) * sizeof(double), stream);
+  plan.cond.alloc(sizeof(double) * 4, stream);
+  double2* part = static_cast<double2*>(plan.partial.p);
+  for (size_t i = 0; i < gt.size(); ++i) {
+    gt[i].partial = part + pend[i].part_off;
+    const int mo = g.out_msg(pend[i].s, pend[i].t);
+    for (int par = 0; par < 2; ++par) {
+      MsgTask m;
+      m.partial = gt[i].partial;
+      m.nchunk = pend[i].nchunk;
+      m.C = pend[i].C;
+      m.out = mptr(1 - par, mo);
+      m.old = mptr(par, mo);
+      m.dist = static_cast<double*>(plan.dist.p) + mo;
+      m.norm_out = nullptr;
+      mt[par].push_back(m);
+    }
+  }
+  upload_vec(plan.gram_tasks, gt, stream);
+  upload_vec(plan.gram_begins, gbeg, stream);
+  upload_vec(plan.msg_tasks[0], mt[0], stream);
+  upload_vec(plan.msg_tasks[1], mt[1], stream);
+  plan.gram_ntask = (int)gt.size();
+  plan.gram_nblocks = nb;
+  plan.nmsg = (int)mt[0].size();
+  plan.valid = true;
+  CK(cudaStreamSynchronize(stream));
+  check_budget();
+}
+
+template <typename R>
+void Job::launch_sweep_kernels(int par) {
+  for (auto& lv : plan.levels) {
+    if (lv.ntask == 0) continue;
+    const size_t smem = (size_t)(kRowTile * (lv.max_din + 1) + lv.max_din * (kColTile + 1)) * sizeof(typename cvec<R>::type);
+    CK(cudaFuncSetAttribute(k_leg_apply<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_leg_apply<R><<<(unsigned)lv.nblocks, kThreads, smem, stream>>>(
+        static_cast<const LegTask*>(lv.tasks[par].p), static_cast<const long long*>(lv.begins.p), lv.ntask,
+        lv.max_din);
+    CK(cudaGetLastError());
+  }
+  k_gram<R><<<(unsigned)plan.gram_nblocks, kThreads, 0, stream>>>(
+      static_cast<const GramTask*>(plan.gram_tasks.p), static_cast<const long long*>(plan.gram_begins.p),
+      plan.gram_ntask);
+  CK(cudaGetLastError());
+  k_msg_finalize<R><<<plan.nmsg, kThreads, 0, stream>>>(static_cast<const MsgTask*>(plan.msg_tasks[par].p));
+  CK(cudaGetLastError());
+  k_sum_scaled<<<1, kThreads, 0, stream>>>(static_cast<const double*>(plan.dist.p), plan.nmsg,
+                                           1.0 / (2.0 * (double)g.edges.size()),
+                                           static_cast<double*>(plan.cond.p));
+  CK(cudaGetLastError());
+}
+
+void Job::run_sweep(int par) {
+  if (!plan.valid) build_plan();
+  if (!plan.graph_exec[par]) {
+    // warm the function attributes outside capture, then capture once
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      if (prec == TNBP_C128) launch_sweep_kernels<double>(par);
+      else launch_sweep_kernels<float>(par);
+    } catch (...) {
+      cudaStreamEndCapture(stream, &graph);
+      throw;
+    }
+    CK(cudaStreamEndCapture(stream, &graph));
+    CK(cudaGraphInstantiate(&plan.graph_exec[par], graph, 0));
+    cudaGraphDestroy(graph);
+  }
+  CK(cudaEventRecord(ev0, stream));
+  CK(cudaGraphLaunch(plan.graph_exec[par], stream));
+  CK(cudaEventRecord(ev1, stream));
+  sweeps_run++;
+}
+
+double Job::read_cond() {
+  CK(cudaMemcpyAsync(host_scalar, plan.cond.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) last_sweep_ms = ms;
+  return host_scalar[0];
+}
+
+void Job::bp_sweep() {
+  run_sweep(cur);
+  cur = 1 - cur;
+  CK(cudaStreamSynchronize(stream));
+}
+
+double Job::bp_condition() {
+  run_sweep(cur);  // writes the other arena; state (cur) unchanged
+  return read_cond();
+}
+
+void Job::bp_run(double tol, int max_iter, int* iters, double* cond) {
+  *iters = 0;
+  *cond = std::nan("");
+  if (max_iter <= 0) return;
+  run_sweep(cur);
+  cur = 1 - cur;
+  *iters = 1;
+  while (true) {
+    run_sweep(cur);
+    const double c = read_cond();
+    *cond = c;
+    if (c < tol) break;
+    if (*iters >= max_iter) break;
+    cur = 1 - cur;
+    ++*iters;
+  }
+}
+
+// --------------------------------------------------------------- AbsorbTPO
+Tpo::~Tpo() {}
+
+void Job::absorb_tpo(const Tpo& tpo) {
+  const int ns = (int)g.labels.size();
+  const int ne = (int)g.edges.size();
+  if ((int)tpo.rank.size() != ne) throw Error(TNBP_EINVAL, "TPO edge count mismatch");
+  std::vector<int> ndim(ne);
+  for (int e = 0; e < ne; ++e) ndim[e] = dim[e] * tpo.rank[e];
+  const std::vector<int> odim = dim;
+  const std::vector<size_t> ovoff = voff, omoff = moff;
+  // new layout
+  dim = ndim;
+  layout();
+  DevBuf nV, nM0, nM1;
+  nV.alloc(v_elems * esz, stream);
+  nM0.alloc(m_elems * esz, stream);
+  nM1.alloc(m_elems * esz, stream);
+  std::vector<AbsorbTask> at;
+  std::vector<long long> ab;
+  long long nb = 0;
+  for (int s = 0; s < ns; ++s) {
+    AbsorbTask t{};
+    t.V = static_cast<char*>(V.p) + ovoff[s] * esz;
+    t.out = static_cast<char*>(nV.p) + voff[s] * esz;
+    t.O = static_cast<const double2*>(tpo.ops.p) + tpo.op_offset[s];
+    t.g = (int)g.legs[s].size();
+    t.d = pd[s];
+    t.dout = tpo.dout[s];
+    for (int k = 0; k < t.g; ++k) { t.Dv[k] = odim[g.legs[s][k]]; t.r[k] = tpo.rank[g.legs[s][k]]; }
+    t.n_out = (long long)site_elems(s);
+    t.block_begin = nb;
+    ab.push_back(nb);
+    nb += (t.n_out + kThreads - 1) / kThreads;
+    at.push_back(t);
+  }
+  std::vector<MsgExpandTask> mt;
+  std::vector<long long> mb;
+  long long nmb = 0;
+  for (int m = 0; m < 2 * ne; ++m) {
+    MsgExpandTask t;
+    t.E = static_cast<char*>(M[cur].p) + omoff[m] * esz;
+    t.out = static_cast<char*>(nM0.p) + moff[m] * esz;
+    t.D = odim[m % ne];
+    t.r = tpo.rank[m % ne];
+    t.block_begin = nmb;
+    mb.push_back(nmb);
+    const long long N = (long long)t.D * t.r;
+    nmb += (N * N + kThreads - 1) / kThreads;
+    mt.push_back(t);
+  }
+  DevBuf dat, dab, dmt, dmb;
+  upload_vec(dat, at, stream);
+  upload_vec(dab, ab, stream);
+  upload_vec(dmt, mt, stream);
+  upload_vec(dmb, mb, stream);
+  if (prec == TNBP_C128) {
+    k_absorb_sites<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<AbsorbTask*>(dat.p), static_cast<long long*>(dab.p), (int)at.size());
+    k_expand_msgs<double><<<(unsigned)nmb, kThreads, 0, stream>>>(static_cast<MsgExpandTask*>(dmt.p), static_cast<long long*>(dmb.p), (int)mt.size());
+  } else {
+    k_absorb_sites<float><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<AbsorbTask*>(dat.p), static_cast<long long*>(dab.p), (int)at.size());
+    k_expand_msgs<float><<<(unsigned)nmb, kThreads, 0, stream>>>(static_cast<MsgExpandTask*>(dmt.p), static_cast<long long*>(dmb.p), (int)mt.size());
+  }
+  CK(cudaGetLastError());
+  std::swap(V, nV);
+  std::swap(M[0], nM0);
+  std::swap(M[1], nM1);
+  cur = 0;
+  plan.valid = false;
+  destroy_graphs();
+  plan = SweepPlan();
+  CK(cudaStreamSynchronize(stream));
+  check_budget();
+}
+
+// ------------------------------------------------- generic leg-apply helper
+// Applies, for every entry, a chain of leg contractions to a site tensor and
+// writes the result to dst.  Used by truncation (projectors) and
+// measurement (incoming messages).
+struct ChainEntry {
+  int site;
+  const void* src;
+  void* dst;                        // final output
+  std::vector<int> legs;            // legs to contract, in order
+  std::vector<const void*> mats;    // Din x Dout matrices (storage precision)
+  std::vector<int> dout;            // output dims
+};
+
+void Job::run_chains(std::vector<ChainEntry>& chains) {
+  if (chains.empty()) return;
+  size_t maxlen = 0;
+  std::vector<size_t> base(chains.size());
+  size_t tot = 0;
+  for (size_t i = 0; i < chains.size(); ++i) {
+    auto sh = site_shape(chains[i].site);
+    size_t n = site_elems(chains[i].site), mx = n;
+    for (size_t k = 0; k < chains[i].legs.size(); ++k) {
+      n = n / sh[chains[i].legs[k]] * chains[i].dout[k];
+      sh[chains[i].legs[k]] = chains[i].dout[k];
+      mx = std::max(mx, n);
+    }
+    base[i] = tot;
+    tot += align_elems(mx);
+    maxlen = std::max(maxlen, chains[i].legs.size());
+  }
+  DevBuf buf[2];
+  buf[0].alloc(std::max<size_t>(tot, 32) * esz, stream);
+  buf[1].alloc(std::max<size_t>(tot, 32) * esz, stream);
+  for (size_t lv = 0; lv < maxlen; ++lv) {
+    std::vector<LegTask> t;
+    std::vector<long long> b;
+    long long nb = 0;
+    int maxdin = 1;
+    for (size_t i = 0; i < chains.size(); ++i) {
+      auto& c = chains[i];
+      if (lv >= c.legs.size()) continue;
+      auto sh = site_shape(c.site);
+      for (size_t k = 0; k < lv; ++k) sh[c.legs[k]] = c.dout[k];
+      const int leg = c.legs[lv];
+      long long L = 1, R = 1;
+      for (int k = 0; k < leg; ++k) L *= sh[k];
+      for (size_t k = leg + 1; k < sh.size(); ++k) R *= sh[k];
+      LegTask lt;
+      lt.in = lv == 0 ? c.src : static_cast<char*>(buf[(lv - 1) & 1].p) + base[i] * esz;
+      lt.out = (lv + 1 == c.legs.size()) ? c.dst : static_cast<char*>(buf[lv & 1].p) + base[i] * esz;
+      lt.mat = c.mats[lv];
+      lt.L = L; lt.R = R; lt.Din = sh[leg]; lt.Dout = c.dout[lv];
+      lt.block_begin = nb;
+      b.push_back(nb);
+      nb += (L * R + kRowTile - 1) / kRowTile;
+      maxdin = std::max(maxdin, lt.Din);
+      t.push_back(lt);
+    }
+    DevBuf dt, db;
+    upload_vec(dt, t, stream);
+    upload_vec(db, b, stream);
+    if (prec == TNBP_C128) {
+      const size_t smem = (size_t)(kRowTile * (maxdin + 1) + maxdin * (kColTile + 1)) * 16;
+      CK(cudaFuncSetAttribute(k_leg_apply<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_leg_apply<double><<<(unsigned)nb, kThreads, smem, stream>>>(static_cast<LegTask*>(dt.p), static_cast<long long*>(db.p), (int)t.size(), maxdin);
+    } else {
+      const size_t smem = (size_t)(kRowTile * (maxdin + 1) + maxdin * (kColTile + 1)) * 8;
+      CK(cudaFuncSetAttribute(k_leg_apply<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_leg_apply<float><<<(unsigned)nb, kThreads, smem, stream>>>(static_cast<LegTask*>(dt.p), static_cast<long long*>(db.p), (int)t.size(), maxdin);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream));
+  }
+}
+
+// --------------------------------------------------------------- truncation
+void Job::truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_out) {
+  if (chi_max < 1) throw Error(TNBP_EINVAL, "chi_max must be >= 1");
+  const int ns = (int)g.labels.size();
+  const int ne = (int)g.edges.size();
+  // per-edge scratch
+  std::vector<size_t> woff(ne), poff(ne), soff(ne);
+  size_t wtot = 0, ptot = 0, stot = 0;
+  for (int e = 0; e < ne; ++e) {
+    const size_t nn = (size_t)dim[e] * dim[e];
+    woff[e] = wtot; wtot += 8 * nn;
+    poff[e] = ptot; ptot += align_elems(nn);
+    soff[e] = stot; stot += (size_t)dim[e];
+  }
+  DevBuf work, sv, perm, Pa, Pb, skeep, keep, err, status;
+  work.alloc(wtot * sizeof(double2), stream);
+  sv.alloc(3 * stot * sizeof(double), stream);
+  perm.alloc(3 * stot * sizeof(int), stream);
+  Pa.alloc(ptot * esz, stream);
+  Pb.alloc(ptot * esz, stream);
+  skeep.alloc(stot * sizeof(double), stream);
+  keep.alloc(ne * sizeof(int), stream);
+  err.alloc(ne * sizeof(double), stream);
+  status.alloc(ne * sizeof(int), stream);
+  std::vector<TruncTask> tt(ne);
+  for (int e = 0; e < ne; ++e) {
+    TruncTask& t = tt[e];
+    t.Ma = mptr(cur, e);
+    t.Mb = mptr(cur, e + ne);
+    t.D = dim[e];
+    t.work = static_cast<double2*>(work.p) + woff[e];
+    t.sv = static_cast<double*>(sv.p) + 3 * soff[e];
+    t.perm = static_cast<int*>(perm.p) + 3 * soff[e];
+    t.Pa = static_cast<char*>(Pa.p) + poff[e] * esz;
+    t.Pb = static_cast<char*>(Pb.p) + poff[e] * esz;
+    t.s_keep = static_cast<double*>(skeep.p) + soff[e];
+    t.keep_out = static_cast<int*>(keep.p) + e;
+    t.err_out = static_cast<double*>(err.p) + e;
+    t.status = static_cast<int*>(status.p) + e;
+  }
+  DevBuf dtt;
+  upload_vec(dtt, tt, stream);
+  if (prec == TNBP_C128) k_truncate_edges<double><<<ne, kThreads, 0, stream>>>(static_cast<TruncTask*>(dtt.p), chi_max, sv_min);
+  else k_truncate_edges<float><<<ne, kThreads, 0, stream>>>(static_cast<TruncTask*>(dtt.p), chi_max, sv_min);
+  CK(cudaGetLastError());
+  std::vector<int> hkeep(ne), hstatus(ne);
+  std::vector<double> herr(ne);
+  CK(cudaMemcpyAsync(hkeep.data(), keep.p, ne * sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CK(cudaMemcpyAsync(herr.data(), err.p, ne * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  CK(cudaMemcpyAsync(hstatus.data(), status.p, ne * sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  // new site tensors: V_s x_k P_k for every leg, then normalize
+  const std::vector<int> odim = dim;
+  const std::vector<size_t> ovoff = voff;
+  dim.assign(hkeep.begin(), hkeep.end());
+  layout();
+  DevBuf nV;
+  nV.alloc(v_elems * esz, stream);
+  std::vector<ChainEntry> chains;
+  {
+    const std::vector<int> ndim = dim;
+    dim = odim;  // site_shape() inside run_chains must see the old dims
+    std::vector<size_t> nvoff = voff;
+    for (int s = 0; s < ns; ++s) {
+      ChainEntry c;
+      c.site = s;
+      c.src = static_cast<char*>(V.p) + ovoff[s] * esz;
+      c.dst = static_cast<char*>(nV.p) + nvoff[s] * esz;
+      for (size_t k = 0; k < g.legs[s].size(); ++k) {
+        const int e = g.legs[s][k];
+        c.legs.push_back((int)k);
+        c.mats.push_back(static_cast<char*>(g.site_a[e] == s ? Pa.p : Pb.p) + poff[e] * esz);
+        c.dout.push_back(ndim[e]);
+      }
+      chains.push_back(c);
+    }
+    run_chains(chains);
+    dim = ndim;
+    voff = nvoff;
+  }
+  std::swap(V, nV);
+  nV.release();
+  normalize_sites();
+  // messages = diag(s)
+  DevBuf nM0, nM1;
+  nM0.alloc(m_elems * esz, stream);
+  nM1.alloc(m_elems * esz, stream);
+  std::vector<DiagTask> dt;
+  for (int m = 0; m < 2 * ne; ++m) {
+    DiagTask t;
+    t.s = static_cast<double*>(skeep.p) + soff[m % ne];
+    t.out = static_cast<char*>(nM0.p) + moff[m] * esz;
+    t.n = dim[m % ne];
+    dt.push_back(t);
+  }
+  DevBuf ddt;
+  upload_vec(ddt, dt, stream);
+  if (prec == TNBP_C128) k_write_diag<double><<<2 * ne, 128, 0, stream>>>(static_cast<DiagTask*>(ddt.p));
+  else k_write_diag<float><<<2 * ne, 128, 0, stream>>>(static_cast<DiagTask*>(ddt.p));
+  CK(cudaGetLastError());
+  std::swap(M[0], nM0);
+  std::swap(M[1], nM1);
+  cur = 0;
+  plan.valid = false;
+  destroy_graphs();
+  plan = SweepPlan();
+  CK(cudaStreamSynchronize(stream));
+  if (dims_out) for (int e = 0; e < ne; ++e) dims_out[e] = hkeep[e];
+  if (err_out) for (int e = 0; e < ne; ++e) err_out[e] = herr[e];
+  int bad = 0;
+  for (int e = 0; e < ne; ++e) bad += hstatus[e] != 0;
+  if (bad) throw Error(TNBP_ENOTCONV, std::to_string(bad) + " edge SVD(s) reached the Jacobi sweep limit");
+  check_budget();
+}
+
+void Job::normalize_sites() {
+  const int ns = (int)g.labels.size();
+  const int per_thread = 8;
+  std::vector<RangeTask> rt;
+  std::vector<long long> rb;
+  long long nb = 0;
+  size_t npart = 0;
+  for (int s = 0; s < ns; ++s) {
+    RangeTask t;
+    t.data = vptr(s);
+    t.n = (long long)site_elems(s);
+    t.nblocks = (int)((t.n + (long long)kThreads * per_thread - 1) / ((long long)kThreads * per_thread));
+    t.block_begin = nb;
+    t.partial = reinterpret_cast<double*>(npart);  // patched below
+    rb.push_back(nb);
+    nb += t.nblocks;
+    npart += t.nblocks;
+    rt.push_back(t);
+  }
+  DevBuf part;
+  part.alloc(npart * sizeof(double), stream);
+  for (auto& t : rt) t.partial = static_cast<double*>(part.p) + reinterpret_cast<size_t>(t.partial);
+  DevBuf drt, drb;
+  upload_vec(drt, rt, stream);
+  upload_vec(drb, rb, stream);
+  if (prec == TNBP_C128) {
+    k_sumsq_partial<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<RangeTask*>(drt.p), static_cast<long long*>(drb.p), ns, per_thread);
+    k_scale_ranges<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<RangeTask*>(drt.p), static_cast<long long*>(drb.p), ns, per_thread);
+  } else {
+    k_sumsq_partial<float><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<RangeTask*>(drt.p), static_cast<long long*>(drb.p), ns, per_thread);
+    k_scale_ranges<float><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<RangeTask*>(drt.p), static_cast<long long*>(drb.p), ns, per_thread);
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(stream));
+}
+
+// -------------------------------------------------------------- measurement
+// Reduced density matrices: one-site rho over the physical leg
+// (measure.h:46-89), two-site environments over (target leg, physical leg)
+// (measure.h:168-245).  Returns device buffers holding FP64 matrices.
+void Job::compute_envs(const std::vector<int>& sites1, const std::vector<std::pair<int, int>>& sidelegs,
+                       DevBuf& out1, DevBuf& out2, std::vector<size_t>& off2) {
+  const int ne = (int)g.edges.size();
+  (void)ne;
+  // W = V x (incoming messages on the selected legs)
+  struct Req { int site; int keep_leg; };  // keep_leg = -1: absorb all legs
+  std::vector<Req> reqs;
+  for (int s : sites1) reqs.push_back({s, -1});
+  for (auto& p : sidelegs) reqs.push_back({p.first, p.second});
+  std::vector<size_t> woff(reqs.size());
+  size_t wtot = 0;
+  for (size_t i = 0; i < reqs.size(); ++i) { woff[i] = wtot; wtot += align_elems(site_elems(reqs[i].site)); }
+  DevBuf W;
+  W.alloc(std::max<size_t>(wtot, 32) * esz, stream);
+  std::vector<ChainEntry> chains;
+  std::vector<size_t> copy_only;
+  for (size_t i = 0; i < reqs.size(); ++i) {
+    ChainEntry c;
+    c.site = reqs[i].site;
+    c.src = vptr(c.site);
+    c.dst = static_cast<char*>(W.p) + woff[i] * esz;
+    const auto sh = site_shape(c.site);
+    for (size_t k = 0; k < g.legs[c.site].size(); ++k) {
+      if ((int)k == reqs[i].keep_leg) continue;
+      c.legs.push_back((int)k);
+      c.mats.push_back(mptr(cur, g.in_msg(c.site, (int)k)));
+      c.dout.push_back(sh[k]);
+    }
+    if (c.legs.empty()) copy_only.push_back(i);
+    else chains.push_back(c);
+  }
+  for (size_t i : copy_only)
+    CK(cudaMemcpyAsync(static_cast<char*>(W.p) + woff[i] * esz, vptr(reqs[i].site), site_elems(reqs[i].site) * esz,
+                       cudaMemcpyDeviceToDevice, stream));
+  run_chains(chains);
+  // Gram partials
+  std::vector<GramTask> gt;
+  std::vector<long long> gb;
+  std::vector<PartialSumTask> pt;
+  long long nb = 0;
+  size_t ptot = 0, o1 = 0, o2 = 0;
+  std::vector<size_t> poff;
+  std::vector<size_t> ooff;
+  off2.clear();
+  for (size_t i = 0; i < reqs.size(); ++i) {
+    const int s = reqs[i].site;
+    const auto sh = site_shape(s);
+    const int gs = (int)g.legs[s].size();
+    GramTask t;
+    t.A = static_cast<char*>(W.p) + woff[i] * esz;
+    t.B = vptr(s);
+    if (reqs[i].keep_leg < 0) {
+      long long L = 1;
+      for (int k = 0; k < gs; ++k) L *= sh[k];
+      t.L = L; t.M = 1; t.D = sh[gs]; t.P = 1;
+    } else {
+      const int kl = reqs[i].keep_leg;
+      long long L = 1, M = 1;
+      for (int k = 0; k < kl; ++k) L *= sh[k];
+      for (int k = kl + 1; k < gs; ++k) M *= sh[k];
+      t.L = L; t.M = M; t.D = sh[kl]; t.P = sh[gs];
+    }
+    t.C = t.D * t.P;
+    t.ctiles = (t.C + kColTile - 1) / kColTile;
+    t.Q = t.L * t.M;
+    long long cr = ((t.Q / 16) + kRowTile - 1) / kRowTile * kRowTile;
+    t.chunk_rows = std::max<long long>(256, std::min<long long>(4096, cr));
+    t.nchunk = (int)((t.Q + t.chunk_rows - 1) / t.chunk_rows);
+    t.block_begin = nb;
+    gb.push_back(nb);
+    nb += (long long)t.nchunk * t.ctiles * t.ctiles;
+    poff.push_back(ptot);
+    ptot += (size_t)t.nchunk * t.C * t.C;
+    if (reqs[i].keep_leg < 0) { ooff.push_back(o1); o1 += (size_t)t.C * t.C; }
+    else { ooff.push_back(o2); off2.push_back(o2); o2 += (size_t)t.C * t.C; }
+    gt.push_back(t);
+  }
+  DevBuf part;
+  part.alloc(std::max<size_t>(ptot, 1) * sizeof(double2), stream);
+  out1.alloc(std::max<size_t>(o1, 1) * sizeof(double2), stream);
+  out2.alloc(std::max<size_t>(o2, 1) * sizeof(double2), stream);
+  for (size_t i = 0; i < gt.size(); ++i) {
+    gt[i].partial = static_cast<double2*>(part.p) + poff[i];
+    PartialSumTask p;
+    p.partial = gt[i].partial;
+    p.nchunk = gt[i].nchunk;
+    p.n = gt[i].C * gt[i].C;
+    p.out = static_cast<double2*>(reqs[i].keep_leg < 0 ? out1.p : out2.p) + ooff[i];
+    pt.push_back(p);
+  }
+  DevBuf dgt, dgb, dpt;
+  upload_vec(dgt, gt, stream);
+  upload_vec(dgb, gb, stream);
+  upload_vec(dpt, pt, stream);
+  if (!gt.empty()) {
+    if (prec == TNBP_C128) k_gram<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<GramTask*>(dgt.p), static_cast<long long*>(dgb.p), (int)gt.size());
+    else k_gram<float><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<GramTask*>(dgt.p), static_cast<long long*>(dgb.p), (int)gt.size());
+    CK(cudaGetLastError());
+    k_partial_sum<<<(unsigned)pt.size(), kThreads, 0, stream>>>(static_cast<PartialSumTask*>(dpt.p));
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(stream));
+}
+
+void Job::measure_terms(const std::vector<TermSpec>& terms, double* values, double* sum) {
+  // distinct one-site requests and two-site sides
+  std::vector<int> sites1;
+  std::map<int, int> pos1;
+  std::vector<std::pair<int, int>> sides;
+  std::map<std::pair<int, int>, int> pos2;
+  struct Where { int a, b, edge; };
+  std::vector<Where> where(terms.size());
+  for (size_t i = 0; i < terms.size(); ++i) {
+    const auto& t = terms[i];
+    if (t.kind == 1) {
+      if (!pos1.count(t.site_a)) { pos1[t.site_a] = (int)sites1.size(); sites1.push_back(t.site_a); }
+    } else {
+      const int e = t.edge;
+      const std::pair<int, int> sa{g.site_a[e], g.leg_a[e]}, sb{g.site_b[e], g.leg_b[e]};
+      if (!pos2.count(sa)) { pos2[sa] = (int)sides.size(); sides.push_back(sa); }
+      if (!pos2.count(sb)) { pos2[sb] = (int)sides.size(); sides.push_back(sb); }
+    }
+  }
+  DevBuf r1, r2;
+  std::vector<size_t> off2;
+  compute_envs(sites1, sides, r1, r2, off2);
+  std::vector<TermTask> tt(terms.size());
+  for (size_t i = 0; i < terms.size(); ++i) {
+    const auto& t = terms[i];
+    TermTask& k = tt[i];
+    k.kind = t.kind;
+    k.coeff = make_double2(t.coeff[0], t.coeff[1]);
+    for (int j = 0; j < 16; ++j) k.op[j] = make_double2(t.op[2 * j], t.op[2 * j + 1]);
+    if (t.kind == 1) {
+      k.d = pd[t.site_a];
+      k.D = 1;
+      size_t off = 0;
+      for (int q = 0; q < pos1[t.site_a]; ++q) off += (size_t)pd[sites1[q]] * pd[sites1[q]];
+      k.rho_a = static_cast<const double2*>(r1.p) + off;
+      k.rho_b = nullptr;
+    } else {
+      const int e = t.edge;
+      // measure.h:126-127: site a = first label of the requested pair
+      const bool flip = g.labels[g.site_a[e]] != t.label_a;
+      const std::pair<int, int> sa{g.site_a[e], g.leg_a[e]}, sb{g.site_b[e], g.leg_b[e]};
+      const auto& A = flip ? sb : sa;
+      const auto& B = flip ? sa : sb;
+      k.d = pd[A.first];
+      k.D = dim[e];
+      k.rho_a = static_cast<const double2*>(r2.p) + off2[pos2[A]];
+      k.rho_b = static_cast<const double2*>(r2.p) + off2[pos2[B]];
+    }
+  }
+  DevBuf dtt, dvals, dsum;
+  upload_vec(dtt, tt, stream);
+  dvals.alloc(std::max<size_t>(terms.size(), 1) * sizeof(double2), stream);
+  dsum.alloc(sizeof(double2), stream);
+  if (!tt.empty()) {
+    k_terms<<<(unsigned)tt.size(), kThreads, 0, stream>>>(static_cast<TermTask*>(dtt.p), static_cast<double2*>(dvals.p));
+    k_weighted_sum<<<1, kThreads, 0, stream>>>(static_cast<TermTask*>(dtt.p), static_cast<double2*>(dvals.p), (int)tt.size(), static_cast<double2*>(dsum.p));
+    CK(cudaGetLastError());
+  }
+  std::vector<double> hv(2 * std::max<size_t>(terms.size(), 1), 0.0);
+  double hs[2] = {0.0, 0.0};
+  if (!tt.empty()) {
+    CK(cudaMemcpyAsync(hv.data(), dvals.p, terms.size() * sizeof(double2), cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(hs, dsum.p, sizeof(double2), cudaMemcpyDeviceToHost, stream));
+  }
+  CK(cudaStreamSynchronize(stream));
+  if (values) std::memcpy(values, hv.data(), terms.size() * 2 * sizeof(double));
+  if (sum) { sum[0] = hs[0]; sum[1] = hs[1]; }
+}
+
+int Job::edge_of(int la, int lb) const {
+  auto ia = g.index_of.find(la), ib = g.index_of.find(lb);
+  if (ia == g.index_of.end() || ib == g.index_of.end()) return -1;
+  for (int e : g.legs[ia->second]) {
+    if ((g.site_a[e] == ia->second && g.site_b[e] == ib->second) ||
+        (g.site_b[e] == ia->second && g.site_a[e] == ib->second))
+      return e;
+  }
+  return -1;
+}
+
+}  // namespace tnbp

@@ -1,0 +1,151 @@
+// Internal declarations of the device engine (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace tnbp {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+extern thread_local std::string g_last_error;
+void check_cuda(cudaError_t e, const char* what, const char* file, int line);
+#define CK(x) ::tnbp::check_cuda((x), #x, __FILE__, __LINE__)
+
+// Stream-ordered device allocation owned by one object.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaStream_t stream = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept { *this = std::move(o); }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p; bytes = o.bytes; stream = o.stream;
+      o.p = nullptr; o.bytes = 0;
+    }
+    return *this;
+  }
+  ~DevBuf();
+  void release();
+  void alloc(size_t nbytes, cudaStream_t s);
+};
+
+// Lattice bookkeeping of graph.h: sorted site labels, incident edges per
+// site in edge order (the leg order of every site tensor).
+struct Graph {
+  std::vector<std::pair<int, int>> edges;
+  std::vector<int> labels;
+  std::map<int, int> index_of;
+  std::vector<std::vector<int>> legs;
+  std::vector<int> site_a, site_b, leg_a, leg_b;
+  Graph() = default;
+  Graph(const int32_t* e, int64_t n);
+  int out_msg(int s, int k) const;
+  int in_msg(int s, int k) const;
+};
+
+struct LevelTasks {
+  DevBuf tasks[2];
+  DevBuf begins;
+  int ntask = 0;
+  long long nblocks = 0;
+  int max_din = 1;
+};
+
+struct SweepPlan {
+  bool valid = false;
+  DevBuf scratch, partial, dist, cond;
+  std::vector<LevelTasks> levels;
+  DevBuf gram_tasks, gram_begins, msg_tasks[2];
+  int gram_ntask = 0, nmsg = 0;
+  long long gram_nblocks = 0;
+  cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+  double flops = 0.0, bytes_alg = 0.0;
+  SweepPlan() = default;
+  SweepPlan(SweepPlan&&) = default;
+  SweepPlan& operator=(SweepPlan&&) = default;
+  ~SweepPlan();
+  uint64_t bytes() const;
+};
+
+// A TPO layer on the device: complex128 op tensors of shape
+// (r_leg0..r_leg{g-1}, d, d') per site.
+struct Tpo {
+  std::vector<int> rank;          // per edge
+  std::vector<int64_t> op_offset; // per site, complex elements
+  std::vector<int> dout;          // per site
+  DevBuf ops;
+  ~Tpo();
+};
+
+struct TermSpec {
+  int kind;          // 1 or 2
+  int site_a;        // kind 1: site index
+  int edge;          // kind 2: edge index
+  int label_a;       // kind 2: label of the first operator's site
+  double op[32];     // reference layout, interleaved complex
+  double coeff[2];
+};
+
+struct ChainEntry;
+
+struct Job {
+  Graph g;
+  int prec;
+  size_t esz;
+  uint64_t budget;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double* host_scalar = nullptr;
+  std::vector<int> pd, dim;
+  std::vector<size_t> voff, moff;
+  size_t v_elems = 0, m_elems = 0;
+  DevBuf V, M[2];
+  int cur = 0;
+  SweepPlan plan;
+  long long sweeps_run = 0;
+  float last_sweep_ms = 0.f;
+
+  Job(const int32_t* e, int64_t n, const int32_t* pdims, int precision, cudaStream_t s, uint64_t budget);
+  ~Job();
+  std::vector<int> site_shape(int s) const;
+  size_t site_elems(int s) const;
+  void layout();
+  void put_complex(DevBuf& dst, const double* src, size_t n, size_t elem_off);
+  void get_complex(const DevBuf& src, double* dst, size_t n, size_t elem_off);
+  uint64_t device_bytes() const;
+  void check_budget() const;
+  void* vptr(int s) const;
+  void* mptr(int arena, int m) const;
+  void destroy_graphs();
+  void build_plan();
+  template <typename R> void launch_sweep_kernels(int par);
+  void run_sweep(int par);
+  double read_cond();
+  void bp_sweep();
+  double bp_condition();
+  void bp_run(double tol, int max_iter, int* iters, double* cond);
+  void absorb_tpo(const Tpo& tpo);
+  void run_chains(std::vector<ChainEntry>& chains);
+  void truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_out);
+  void normalize_sites();
+  void compute_envs(const std::vector<int>& sites1, const std::vector<std::pair<int, int>>& sidelegs,
+                    DevBuf& out1, DevBuf& out2, std::vector<size_t>& off2);
+  void measure_terms(const std::vector<TermSpec>& terms, double* values, double* sum);
+  int edge_of(int la, int lb) const;
+};
+
+}  // namespace tnbp

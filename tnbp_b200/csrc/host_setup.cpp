@@ -1,0 +1,973 @@
+// Host-side problem builders of the estimator path, written for this
+// engine: lattice and edge bookkeeping, OpenQASM 2 / 3-subset parsing,
+// sparse-Pauli parsing and classification, and TPO (tensor-product
+// operator) construction.  Their outputs (edge order, leg order, layer
+// split, gate order, Pauli qubit order, kept terms) are required to be
+// identical to the reference's; numeric TPO factors may differ by a gauge
+// on the operator bonds (a different but equally valid SVD), which leaves
+// every observable unchanged.
+#include "host_setup.h"
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <complex>
+#include <cstdlib>
+#include <map>
+#include <numeric>
+#include <queue>
+#include <set>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <unordered_set>
+#include <vector>
+
+namespace tnbp_host {
+
+using cd = std::complex<double>;
+
+// ------------------------------------------------------------- lattice
+// bond_square_lattice (include/tnbp/lattice/square.h:14-34): row-major sites
+// ix + Lx*iy, per site the right neighbour then the one below.
+Edges square_lattice(int Lx, int Ly) {
+  if (Lx < 1 || Ly < 1) throw HostError(-1, "lattice sides must be >= 1");
+  Edges out;
+  for (int iy = 0; iy < Ly; ++iy)
+    for (int ix = 0; ix < Lx; ++ix) {
+      const int s = ix + Lx * iy;
+      if (ix + 1 < Lx) out.push_back({s, s + 1});
+      if (iy + 1 < Ly) out.push_back({s, s + Lx});
+    }
+  return out;
+}
+
+// GreedyEdgeLayering (graph.h:138-170): repeated first-fit matchings in edge order.
+std::vector<int> greedy_layering(const Edges& e, int* nlayers) {
+  std::vector<int> layer(e.size(), -1);
+  int l = 0;
+  size_t left = e.size();
+  while (left > 0) {
+    std::unordered_set<int> used;
+    for (size_t i = 0; i < e.size(); ++i) {
+      if (layer[i] >= 0) continue;
+      if (used.count(e[i].first) || used.count(e[i].second)) continue;
+      layer[i] = l;
+      used.insert(e[i].first);
+      used.insert(e[i].second);
+      --left;
+    }
+    ++l;
+  }
+  *nlayers = l;
+  return layer;
+}
+
+std::vector<int> surrounding_bonds(const Edges& e, int site) {
+  std::vector<int> r;
+  for (size_t m = 0; m < e.size(); ++m) {
+    if (e[m].first == site) r.push_back((int)m);
+    if (e[m].second == site) r.push_back((int)m);
+  }
+  return r;
+}
+
+std::vector<int> site_labels(const Edges& e) {
+  std::vector<int> s;
+  for (auto& p : e) { s.push_back(p.first); s.push_back(p.second); }
+  std::sort(s.begin(), s.end());
+  s.erase(std::unique(s.begin(), s.end()), s.end());
+  return s;
+}
+
+// FindShortestPath (graph.h:57-108): BFS over compressed labels, neighbours
+// visited in edge-list insertion order; empty if unreachable.
+std::vector<int> shortest_path(const Edges& e, int src, int dst) {
+  const auto sites = site_labels(e);
+  std::unordered_map<int, size_t> idx;
+  for (size_t i = 0; i < sites.size(); ++i) idx[sites[i]] = i;
+  if (!idx.count(src) || !idx.count(dst)) return {};
+  std::vector<std::vector<size_t>> adj(sites.size());
+  for (auto& p : e) { adj[idx[p.first]].push_back(idx[p.second]); adj[idx[p.second]].push_back(idx[p.first]); }
+  const size_t s = idx[src], t = idx[dst];
+  std::vector<char> seen(sites.size(), 0);
+  std::vector<size_t> prev(sites.size(), (size_t)-1);
+  std::queue<size_t> q;
+  q.push(s);
+  seen[s] = 1;
+  while (!q.empty()) {
+    const size_t u = q.front();
+    q.pop();
+    if (u == t) break;
+    for (size_t v : adj[u])
+      if (!seen[v]) { seen[v] = 1; prev[v] = u; q.push(v); }
+  }
+  if (!seen[t]) return {};
+  std::vector<int> path;
+  for (size_t c = t; c != (size_t)-1; c = prev[c]) path.push_back(sites[c]);
+  std::reverse(path.begin(), path.end());
+  return path;
+}
+
+// ---------------------------------------------------------------- QASM
+// Grammar and broadcasting of include/qasm/{common/reader,v2/parser,
+// v3/parser}.h: expressions with + - * / ( ) unary sign, pi and tau, numbers
+// via strtod; a register argument expands to all its qubits; a gate whose
+// argument count is a multiple of its arity is split into consecutive
+// groups; barrier keeps all its qubits in one instruction.
+namespace {
+struct Reader {
+  std::string src;
+  size_t i = 0, line = 1, col = 1;
+  bool eof() const { return i >= src.size(); }
+  char peek() const { return eof() ? '\0' : src[i]; }
+  char get() {
+    if (eof()) return '\0';
+    char c = src[i++];
+    if (c == '\n') { ++line; col = 1; } else ++col;
+    return c;
+  }
+  [[noreturn]] void err(const std::string& m) const {
+    throw HostError(-5, "QASM parse error (" + std::to_string(line) + ":" + std::to_string(col) + "): " + m);
+  }
+  static bool id0(char c) { return std::isalpha((unsigned char)c) || c == '_'; }
+  static bool id1(char c) { return std::isalnum((unsigned char)c) || c == '_' || c == '$'; }
+  void ws() {
+    for (;;) {
+      while (!eof() && std::isspace((unsigned char)peek())) get();
+      if (peek() == '/' && i + 1 < src.size() && src[i + 1] == '/') { while (!eof() && get() != '\n') {} continue; }
+      if (peek() == '/' && i + 1 < src.size() && src[i + 1] == '*') {
+        get(); get();
+        while (!eof()) { char c = get(); if (c == '*' && peek() == '/') { get(); break; } }
+        continue;
+      }
+      break;
+    }
+  }
+  std::string word() {
+    ws();
+    if (!id0(peek())) err("identifier expected");
+    std::string w(1, get());
+    while (id1(peek())) w.push_back(get());
+    return w;
+  }
+  static bool ieq(const std::string& a, const char* b) {
+    size_t n = std::strlen(b);
+    if (a.size() != n) return false;
+    for (size_t k = 0; k < n; ++k)
+      if (std::tolower((unsigned char)a[k]) != std::tolower((unsigned char)b[k])) return false;
+    return true;
+  }
+  bool peek_word(const char* w) {
+    ws();
+    if (!id0(peek())) return false;
+    size_t si = i, sl = line, sc = col;
+    std::string t = word();
+    i = si; line = sl; col = sc;
+    return ieq(t, w);
+  }
+  void expect(char ch) {
+    ws();
+    if (peek() != ch) err(std::string("expected '") + ch + "'");
+    get();
+  }
+  void version() {
+    ws();
+    if (peek() == '"') { get(); while (!eof() && get() != '"') {} return; }
+    while (!eof() && (std::isdigit((unsigned char)peek()) || peek() == '.')) get();
+  }
+  double number() {
+    ws();
+    size_t s = i;
+    bool dot = false, ex = false;
+    if (peek() == '+' || peek() == '-') get();
+    while (!eof()) {
+      char c = peek();
+      if (std::isdigit((unsigned char)c)) get();
+      else if (c == '.' && !dot) { dot = true; get(); }
+      else if ((c == 'e' || c == 'E') && !ex) { ex = true; get(); if (peek() == '+' || peek() == '-') get(); }
+      else break;
+    }
+    if (i == s) err("number expected");
+    return std::strtod(src.substr(s, i - s).c_str(), nullptr);
+  }
+  double factor() {
+    ws();
+    char c = peek();
+    if (c == '(') { get(); double v = expr(); expect(')'); return v; }
+    if (c == '+' || c == '-') { bool neg = c == '-'; get(); double v = factor(); return neg ? -v : v; }
+    if (id0(c)) {
+      std::string w = word();
+      if (ieq(w, "pi")) return 3.14159265358979323846;
+      if (ieq(w, "tau")) return 6.28318530717958647692;
+      err("unknown symbol in expression: " + w);
+    }
+    return number();
+  }
+  double term() {
+    double v = factor();
+    for (;;) {
+      ws();
+      char c = peek();
+      if (c == '*') { get(); v *= factor(); }
+      else if (c == '/') { get(); double d = factor(); if (d == 0.0) err("division by zero"); v /= d; }
+      else break;
+    }
+    return v;
+  }
+  double expr() {
+    double v = term();
+    for (;;) {
+      ws();
+      char c = peek();
+      if (c == '+') { get(); v += term(); }
+      else if (c == '-') { get(); v -= term(); }
+      else break;
+    }
+    return v;
+  }
+  std::vector<double> params() {
+    std::vector<double> p;
+    expect('(');
+    ws();
+    if (peek() != ')') {
+      for (;;) { p.push_back(expr()); ws(); if (peek() == ',') { get(); continue; } break; }
+    }
+    expect(')');
+    return p;
+  }
+};
+
+Op map_gate(const std::string& g) {
+  auto L = [&](const char* s) { return Reader::ieq(g, s); };
+  if (L("u3") || L("u")) return Op::U3;
+  if (L("u2")) return Op::U2;
+  if (L("u1") || L("p")) return Op::U1;
+  if (L("rx")) return Op::RX;
+  if (L("ry")) return Op::RY;
+  if (L("rz")) return Op::RZ;
+  if (L("h")) return Op::H;
+  if (L("x")) return Op::X;
+  if (L("y")) return Op::Y;
+  if (L("z")) return Op::Z;
+  if (L("s")) return Op::S;
+  if (L("sdg")) return Op::SDG;
+  if (L("t")) return Op::T;
+  if (L("tdg")) return Op::TDG;
+  if (L("id")) return Op::ID;
+  if (L("cx") || L("cnot")) return Op::CX;
+  if (L("cz")) return Op::CZ;
+  if (L("swap")) return Op::SWAP;
+  if (L("rzz")) return Op::RZZ;
+  if (L("ccx") || L("toffoli")) return Op::CCX;
+  if (L("cswap")) return Op::CSWAP;
+  return Op::CUSTOM;
+}
+size_t arity(Op op) {
+  switch (op) {
+    case Op::U3: case Op::U2: case Op::U1: case Op::RX: case Op::RY: case Op::RZ: case Op::H:
+    case Op::X: case Op::Y: case Op::Z: case Op::S: case Op::SDG: case Op::T: case Op::TDG: case Op::ID:
+      return 1;
+    case Op::CX: case Op::CZ: case Op::SWAP: case Op::RZZ: return 2;
+    case Op::CCX: case Op::CSWAP: return 3;
+    default: return 0;
+  }
+}
+
+struct Parser {
+  Reader r;
+  bool v3 = false;
+  Program prog;
+  std::unordered_map<std::string, size_t> qsz, csz;
+
+  void check_q(const std::string& reg, size_t idx) {
+    auto it = qsz.find(reg);
+    if (it == qsz.end()) r.err("unknown qreg: " + reg);
+    if (idx >= it->second) r.err("qreg index out of range: " + reg + "[" + std::to_string(idx) + "]");
+  }
+  void check_c(const std::string& reg, size_t idx) {
+    auto it = csz.find(reg);
+    if (it == csz.end()) r.err("unknown creg: " + reg);
+    if (idx >= it->second) r.err("creg index out of range: " + reg + "[" + std::to_string(idx) + "]");
+  }
+  std::vector<QArg> one_qarg() {
+    r.ws();
+    std::string reg = r.word();
+    r.ws();
+    if (r.peek() == '[') {
+      r.get();
+      r.ws();
+      size_t lo = (size_t)r.number();
+      r.ws();
+      if (v3 && r.peek() == ':') {
+        r.get();
+        r.ws();
+        size_t hi = (size_t)r.number();
+        r.expect(']');
+        auto it = qsz.find(reg);
+        if (it == qsz.end()) r.err("unknown qreg: " + reg);
+        if (hi < lo || hi > it->second) r.err("slice out of range");
+        std::vector<QArg> v;
+        for (size_t k = lo; k < hi; ++k) v.push_back({reg, k});
+        return v;
+      }
+      r.expect(']');
+      check_q(reg, lo);
+      return {{reg, lo}};
+    }
+    auto it = qsz.find(reg);
+    if (it == qsz.end()) r.err("unknown qreg: " + reg);
+    std::vector<QArg> v;
+    for (size_t k = 0; k < it->second; ++k) v.push_back({reg, k});
+    return v;
+  }
+  std::vector<QArg> qargs(bool many) {
+    auto out = one_qarg();
+    if (!many) return out;
+    r.ws();
+    while (r.peek() == ',') {
+      r.get();
+      auto nx = one_qarg();
+      out.insert(out.end(), nx.begin(), nx.end());
+      r.ws();
+    }
+    return out;
+  }
+  void push(Op op, std::vector<QArg> q, std::vector<double> p) {
+    Instruction in;
+    in.op = op;
+    in.qubits = std::move(q);
+    in.params = std::move(p);
+    prog.instructions.push_back(std::move(in));
+  }
+  void include() { r.word(); r.ws(); r.expect('"'); while (!r.eof() && r.get() != '"') {} r.expect(';'); }
+  void reg_decl(bool quantum) {  // v2: qreg/creg name[n];
+    r.word();
+    std::string nm = r.word();
+    r.ws();
+    r.expect('[');
+    size_t n = (size_t)r.number();
+    r.expect(']');
+    r.expect(';');
+    (quantum ? qsz : csz)[nm] = n;
+  }
+  void decl_v3(bool quantum) {  // v3: qubit[n] name; / bit[n] name;
+    r.word();
+    r.ws();
+    size_t n = 1;
+    if (r.peek() == '[') { r.get(); n = (size_t)r.number(); r.expect(']'); }
+    std::string nm = r.word();
+    r.expect(';');
+    (quantum ? qsz : csz)[nm] = n;
+  }
+  void barrier() { r.word(); auto q = qargs(true); r.expect(';'); push(Op::BARRIER, q, {}); }
+  void reset() {
+    r.word();
+    auto q = qargs(true);
+    r.expect(';');
+    for (auto& a : q) push(Op::RESET, {a}, {});
+  }
+  std::pair<std::string, size_t> carg() {
+    r.ws();
+    std::string reg = r.word();
+    r.ws();
+    if (v3 && r.peek() != '[') {
+      auto it = csz.find(reg);
+      if (it == csz.end()) r.err("unknown bit/creg: " + reg);
+      if (it->second != 1) r.err("missing index for creg: " + reg);
+      return {reg, 0};
+    }
+    r.expect('[');
+    size_t idx = (size_t)r.number();
+    r.expect(']');
+    check_c(reg, idx);
+    return {reg, idx};
+  }
+  void measure_arrow() {
+    r.word();
+    auto q = qargs(false);
+    r.ws();
+    if (!(r.peek() == '-' && r.i + 1 < r.src.size() && r.src[r.i + 1] == '>')) r.err("expected '->' after measure");
+    r.get(); r.get();
+    carg();
+    r.expect(';');
+    if (q.size() != 1) r.err("measure expects a single qubit");
+    push(Op::MEASURE, {q[0]}, {});
+  }
+  bool looks_bit_assign() {
+    size_t si = r.i, sl = r.line, sc = r.col;
+    r.ws();
+    bool ok = false;
+    if (r.peek_word("bit")) {
+      r.word();
+      r.ws();
+      if (Reader::id0(r.peek())) { r.word(); r.ws(); ok = r.peek() == '='; }
+    }
+    r.i = si; r.line = sl; r.col = sc;
+    return ok;
+  }
+  bool looks_creg_assign() {
+    size_t si = r.i, sl = r.line, sc = r.col;
+    r.ws();
+    bool ok = false;
+    if (Reader::id0(r.peek())) {
+      r.word();
+      r.ws();
+      if (r.peek() == '[') { r.get(); r.number(); r.expect(']'); }
+      r.ws();
+      ok = r.peek() == '=';
+    }
+    r.i = si; r.line = sl; r.col = sc;
+    return ok;
+  }
+  void measure_assign() {
+    r.ws();
+    if (r.peek_word("bit")) {
+      r.word();
+      r.ws();
+      if (r.peek() == '[') r.err("bit array not allowed on LHS with declaration here");
+      std::string nm = r.word();
+      if (!csz.count(nm)) csz[nm] = 1;
+    } else {
+      carg();
+    }
+    r.ws();
+    r.expect('=');
+    r.ws();
+    if (!r.peek_word("measure")) r.err("expected 'measure' in assignment");
+    r.word();
+    auto q = qargs(false);
+    r.expect(';');
+    if (q.size() != 1) r.err("measure expects a single qubit");
+    push(Op::MEASURE, {q[0]}, {});
+  }
+  void gate() {
+    std::string g = r.word();
+    if (v3 && (Reader::ieq(g, "ctrl") || Reader::ieq(g, "inv") || Reader::ieq(g, "pow")))
+      r.err("gate modifiers are not supported in this subset");
+    std::vector<double> p;
+    r.ws();
+    if (r.peek() == '(') p = r.params();
+    r.ws();
+    auto q = qargs(true);
+    r.expect(';');
+    const Op op = map_gate(g);
+    const size_t ar = arity(op);
+    if (ar > 0 && q.size() % ar != 0) r.err("gate '" + g + "' expects multiple of " + std::to_string(ar) + " qubits");
+    if (ar == 0) { push(op, q, p); return; }
+    for (size_t k = 0; k < q.size(); k += ar)
+      push(op, std::vector<QArg>(q.begin() + k, q.begin() + k + ar), p);
+  }
+  Program parse(const std::string& s, bool version3) {
+    r.src = s;
+    v3 = version3;
+    r.ws();
+    if (v3) {
+      if (!r.peek_word("OPENQASM")) r.err("OPENQASM header required for v3");
+      r.word(); r.version(); r.expect(';');
+    } else if (r.peek_word("OPENQASM")) {
+      r.word(); r.version(); r.expect(';');
+    }
+    while (!r.eof()) {
+      r.ws();
+      if (r.eof()) break;
+      if (r.peek_word("include")) { include(); continue; }
+      if (!v3) {
+        if (r.peek_word("qreg")) { reg_decl(true); continue; }
+        if (r.peek_word("creg")) { reg_decl(false); continue; }
+        if (r.peek_word("barrier")) { barrier(); continue; }
+        if (r.peek_word("reset")) { reset(); continue; }
+        if (r.peek_word("measure")) { measure_arrow(); continue; }
+        gate();
+        continue;
+      }
+      if (r.peek_word("qubit")) { decl_v3(true); continue; }
+      if (r.peek_word("barrier")) { barrier(); continue; }
+      if (r.peek_word("reset")) { reset(); continue; }
+      if (r.peek_word("measure")) { measure_arrow(); continue; }
+      if (looks_bit_assign() || looks_creg_assign()) { measure_assign(); continue; }
+      if (r.peek_word("bit")) { decl_v3(false); continue; }
+      {
+        size_t si = r.i, sl = r.line, sc = r.col;
+        std::string w = r.word();
+        if (Reader::ieq(w, "ctrl") || Reader::ieq(w, "inv") || Reader::ieq(w, "pow"))
+          r.err("gate modifiers (ctrl/inv/pow) are not supported in this subset");
+        r.i = si; r.line = sl; r.col = sc;
+      }
+      gate();
+    }
+    return prog;
+  }
+};
+}  // namespace
+
+// parse_any (include/qasm/any.h:8-21): v3 when the 32 characters after
+// "OPENQASM" contain a '3', else v2.
+Program parse_qasm(const std::string& src) {
+  const auto pos = src.find("OPENQASM");
+  bool is3 = false;
+  if (pos != std::string::npos) is3 = src.substr(pos, 32).find('3') != std::string::npos;
+  Parser p;
+  return p.parse(src, is3);
+}
+
+int qubit_count(const Instruction& in) {
+  switch (in.op) {
+    case Op::MEASURE: case Op::RESET: return 1;
+    case Op::BARRIER: case Op::CUSTOM: return (int)in.qubits.size();
+    default: return (int)arity(in.op);
+  }
+}
+
+// EdgesFromQasm (qasmtoedge.h:38-56)
+Edges qasm_edges(const Program& p) {
+  Edges e;
+  for (auto& in : p.instructions) {
+    if (qubit_count(in) != 2) continue;
+    int a = (int)in.qubits[0].index, b = (int)in.qubits[1].index;
+    e.push_back(a < b ? std::make_pair(a, b) : std::make_pair(b, a));
+  }
+  std::sort(e.begin(), e.end());
+  e.erase(std::unique(e.begin(), e.end()), e.end());
+  return e;
+}
+
+// ------------------------------------------------------------ gate matrices
+// U[out][in] in the qubit order of the instruction, state index
+// q0 + 2 q1 (+ 4 q2) (little-endian, as qasmtotpo.h:19-144 encodes them).
+static std::vector<cd> gate_matrix(const Instruction& in) {
+  const double pi = 3.14159265358979323846;
+  auto P = [&](size_t k) { return in.params.size() > k ? in.params[k] : 0.0; };
+  const cd I(0, 1);
+  switch (in.op) {
+    case Op::U3: {
+      const double th = P(0), ph = P(1), la = P(2);
+      return {std::cos(th / 2), -std::exp(I * la) * std::sin(th / 2), std::exp(I * ph) * std::sin(th / 2),
+              std::exp(I * (ph + la)) * std::cos(th / 2)};
+    }
+    case Op::U2: {
+      const double ph = P(0), la = P(1), s = 1 / std::sqrt(2.0);
+      return {s, -std::exp(I * la) * s, std::exp(I * ph) * s, std::exp(I * (ph + la)) * s};
+    }
+    case Op::U1: return {1, 0, 0, std::exp(I * P(0))};
+    case Op::RX: { const double t = P(0); return {std::cos(t / 2), -I * std::sin(t / 2), -I * std::sin(t / 2), std::cos(t / 2)}; }
+    case Op::RY: { const double t = P(0); return {std::cos(t / 2), -std::sin(t / 2), std::sin(t / 2), std::cos(t / 2)}; }
+    case Op::RZ: { const double t = P(0); return {std::exp(-I * (t / 2)), 0, 0, std::exp(I * (t / 2))}; }
+    case Op::H: { const double s = 1 / std::sqrt(2.0); return {s, s, s, -s}; }
+    case Op::X: return {0, 1, 1, 0};
+    case Op::Y: return {0, -I, I, 0};
+    case Op::Z: return {1, 0, 0, -1};
+    case Op::S: return {1, 0, 0, I};
+    case Op::SDG: return {1, 0, 0, -I};
+    case Op::T: return {1, 0, 0, std::exp(I * (pi / 4))};
+    case Op::TDG: return {1, 0, 0, std::exp(-I * (pi / 4))};
+    case Op::ID: return {1, 0, 0, 1};
+    case Op::CX: { std::vector<cd> m(16, 0.0); m[0] = 1; m[2 * 4 + 2] = 1; m[1 * 4 + 3] = 1; m[3 * 4 + 1] = 1; return m; }
+    case Op::CZ: { std::vector<cd> m(16, 0.0); m[0] = 1; m[5] = 1; m[10] = 1; m[15] = -1; return m; }
+    case Op::SWAP: { std::vector<cd> m(16, 0.0); m[0] = 1; m[1 * 4 + 2] = 1; m[2 * 4 + 1] = 1; m[15] = 1; return m; }
+    case Op::RZZ: {
+      const double t = P(0);
+      std::vector<cd> m(16, 0.0);
+      m[0] = std::exp(-I * (t / 2)); m[5] = std::exp(I * (t / 2)); m[10] = std::exp(I * (t / 2)); m[15] = std::exp(-I * (t / 2));
+      return m;
+    }
+    case Op::CCX: {
+      std::vector<cd> m(64, 0.0);
+      for (int i = 0; i < 8; ++i) m[i * 8 + i] = 1;
+      m[3 * 8 + 3] = 0; m[3 * 8 + 7] = 1; m[7 * 8 + 3] = 1; m[7 * 8 + 7] = 0;
+      return m;
+    }
+    case Op::CSWAP: {
+      std::vector<cd> m(64, 0.0);
+      m[0] = 1; m[9] = 1; m[18] = 1; m[45] = 1; m[54] = 1; m[63] = 1; m[3 * 8 + 5] = 1; m[5 * 8 + 3] = 1;
+      return m;
+    }
+    default:
+      throw HostError(-6, "matrix for this op not implemented");
+  }
+}
+
+// ------------------------------------------------------- small dense SVD
+// One-sided Jacobi SVD of an m x n complex matrix (column-major), m >= n
+// handled directly, m < n through the adjoint.  s descending.
+static void small_svd(int m, int n, const std::vector<cd>& A, std::vector<cd>& U, std::vector<double>& s,
+                      std::vector<cd>& Vh) {
+  const bool tall = m >= n;
+  const int M = tall ? m : n, N = tall ? n : m;
+  std::vector<cd> W(M * N);
+  for (int r = 0; r < m; ++r)
+    for (int c = 0; c < n; ++c) {
+      if (tall) W[r + M * c] = A[r + m * c];
+      else W[c + M * r] = std::conj(A[r + m * c]);
+    }
+  std::vector<cd> V(N * N, 0.0);
+  for (int i = 0; i < N; ++i) V[i + N * i] = 1.0;
+  for (int sweep = 0; sweep < 80; ++sweep) {
+    bool rot = false;
+    for (int i = 0; i < N - 1; ++i)
+      for (int j = i + 1; j < N; ++j) {
+        double al = 0, be = 0;
+        cd ga = 0;
+        for (int r = 0; r < M; ++r) {
+          al += std::norm(W[r + M * i]);
+          be += std::norm(W[r + M * j]);
+          ga += std::conj(W[r + M * i]) * W[r + M * j];
+        }
+        const double g = std::abs(ga);
+        if (!(g > 0) || g <= 1e-15 * std::sqrt(al * be)) continue;
+        rot = true;
+        const cd ph = ga / g;
+        const double z = (be - al) / (2 * g);
+        const double t = (z >= 0 ? 1.0 : -1.0) / (std::abs(z) + std::sqrt(1 + z * z));
+        const double c = 1 / std::sqrt(1 + t * t), sn = c * t;
+        for (int r = 0; r < M; ++r) {
+          const cd x = W[r + M * i], y = W[r + M * j];
+          W[r + M * i] = c * x - sn * std::conj(ph) * y;
+          W[r + M * j] = sn * ph * x + c * y;
+        }
+        for (int r = 0; r < N; ++r) {
+          const cd x = V[r + N * i], y = V[r + N * j];
+          V[r + N * i] = c * x - sn * std::conj(ph) * y;
+          V[r + N * j] = sn * ph * x + c * y;
+        }
+      }
+    if (!rot) break;
+  }
+  std::vector<double> sv(N);
+  for (int j = 0; j < N; ++j) {
+    double a = 0;
+    for (int r = 0; r < M; ++r) a += std::norm(W[r + M * j]);
+    sv[j] = std::sqrt(a);
+  }
+  std::vector<int> ord(N);
+  std::iota(ord.begin(), ord.end(), 0);
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return sv[a] > sv[b]; });
+  // worked matrix = L diag(s) R^H with L (M x N), R (N x N)
+  std::vector<cd> L(M * N, 0.0), Rm(N * N);
+  s.assign(N, 0.0);
+  for (int k = 0; k < N; ++k) {
+    const int j = ord[k];
+    s[k] = sv[j];
+    for (int r = 0; r < N; ++r) Rm[r + N * k] = V[r + N * j];
+    if (sv[j] > 0)
+      for (int r = 0; r < M; ++r) L[r + M * k] = W[r + M * j] / sv[j];
+  }
+  if (tall) {
+    U = L;
+    Vh.assign(N * n, 0.0);
+    for (int k = 0; k < N; ++k)
+      for (int c = 0; c < n; ++c) Vh[k + N * c] = std::conj(Rm[c + N * k]);
+  } else {  // A = R diag(s) L^H
+    U = Rm;
+    Vh.assign(N * n, 0.0);
+    for (int k = 0; k < N; ++k)
+      for (int c = 0; c < n; ++c) Vh[k + N * c] = std::conj(L[c + M * k]);
+  }
+}
+
+// ---------------------------------------------------------- TPO building
+// Operator tensor of one site: legs (bond_0..bond_{g-1}, in, out),
+// column-major, entry O[..., in, out] = <out| op |in>.
+struct SiteOp {
+  std::vector<int> shape;  // g bond dims then 2, 2
+  std::vector<cd> data;
+};
+
+static SiteOp identity_op(int g) {
+  SiteOp o;
+  o.shape.assign(g, 1);
+  o.shape.push_back(2);
+  o.shape.push_back(2);
+  o.data = {1.0, 0.0, 0.0, 1.0};
+  return o;
+}
+
+// Apply X after the current operator along bond legs `legs` (X's leading
+// legs, in the given order), merging each (old bond, X leg) pair as
+// old + D_old * x:  new[..., (b, x)..., in, o'] = sum_o T[..., b..., in, o] X[x..., o, o'].
+// X layout: (x_0, ..., x_{k-1}, o_in, o_out) column-major.
+static void attach(SiteOp& T, const std::vector<int>& legs, const std::vector<int>& xdims, const std::vector<cd>& X) {
+  const int g = (int)T.shape.size() - 2;
+  std::vector<int> nshape = T.shape;
+  for (size_t i = 0; i < legs.size(); ++i) nshape[legs[i]] = T.shape[legs[i]] * xdims[i];
+  size_t nx = 1;
+  for (int d : xdims) nx *= d;
+  size_t nb = 1;
+  for (int k = 0; k < g; ++k) nb *= T.shape[k];
+  size_t nnew = 1;
+  for (int d : nshape) nnew *= d;
+  std::vector<cd> out(nnew, 0.0);
+  std::vector<int> bc(g), xc(legs.size());
+  for (size_t b = 0; b < nb; ++b) {
+    size_t t = b;
+    for (int k = 0; k < g; ++k) { bc[k] = (int)(t % T.shape[k]); t /= T.shape[k]; }
+    for (size_t x = 0; x < nx; ++x) {
+      size_t u = x;
+      for (size_t i = 0; i < legs.size(); ++i) { xc[i] = (int)(u % xdims[i]); u /= xdims[i]; }
+      size_t nidx = 0, st = 1;
+      for (int k = 0; k < g; ++k) {
+        int v = bc[k];
+        for (size_t i = 0; i < legs.size(); ++i)
+          if (legs[i] == k) v = bc[k] + T.shape[k] * xc[i];
+        nidx += v * st;
+        st *= nshape[k];
+      }
+      for (int in = 0; in < 2; ++in)
+        for (int o2 = 0; o2 < 2; ++o2) {
+          cd acc = 0;
+          for (int o = 0; o < 2; ++o)
+            acc += T.data[b + nb * (in + 2 * o)] * X[x + nx * (o + 2 * o2)];
+          out[nidx + st * (in + 2 * o2)] += acc;
+        }
+    }
+  }
+  T.shape = nshape;
+  T.data = std::move(out);
+}
+
+// X for a 1-qubit matrix given row-major, list[2 out + in] = U[out][in]:
+// X[o_in + 2 o_out] = U[o_out][o_in] is the same list (the reference's
+// InstructionTensor reads it with address c0 + 2 c1, qasmtotpo.h:177-192).
+static std::vector<cd> one_qubit_x(const std::vector<cd>& U) { return U; }
+
+struct LayerBuilder {
+  const Edges& edges;
+  std::vector<int> sites;
+  std::map<int, int> pos;
+  std::vector<std::vector<int>> bonds;  // per site index: incident edge ids
+  std::vector<SiteOp> ops;
+  LayerBuilder(const Edges& e) : edges(e) {
+    sites = site_labels(e);
+    for (size_t i = 0; i < sites.size(); ++i) pos[sites[i]] = (int)i;
+    bonds.resize(sites.size());
+    for (size_t i = 0; i < sites.size(); ++i) bonds[i] = surrounding_bonds(e, sites[i]);
+    reset();
+  }
+  void reset() {
+    ops.clear();
+    for (size_t i = 0; i < sites.size(); ++i) ops.push_back(identity_op((int)bonds[i].size()));
+  }
+  int site_index(int label) const {
+    auto it = pos.find(label);
+    if (it == pos.end()) throw HostError(-1, "gate on qubit " + std::to_string(label) + " that no 2-qubit gate touches");
+    return it->second;
+  }
+  int leg_toward(int si, int other_label) const {
+    const int me = sites[si];
+    for (size_t k = 0; k < bonds[si].size(); ++k) {
+      const auto& e = edges[bonds[si][k]];
+      if ((e.first == me && e.second == other_label) || (e.second == me && e.first == other_label)) return (int)k;
+    }
+    throw HostError(-1, "no edge between path neighbours");
+  }
+  void one_qubit(int label, const std::vector<cd>& U) {
+    const int si = site_index(label);
+    attach(ops[si], {}, {}, one_qubit_x(U));
+  }
+  // Two-qubit gate on (a, b): operator-Schmidt split with trunc SVD
+  // (chi_max 4, s_min 1e-12, sqrt(s) to both factors), identity
+  // pass-through tensors on intermediate path sites (qasmtotpo.h:287-437).
+  void two_qubit(int qa, int qb, const std::vector<cd>& U) {
+    // G(a_in, a_out ; b_in, b_out) as a 4 x 4 matrix, row a_in + 2 a_out
+    std::vector<cd> G(16);
+    for (int ai = 0; ai < 2; ++ai)
+      for (int ao = 0; ao < 2; ++ao)
+        for (int bi = 0; bi < 2; ++bi)
+          for (int bo = 0; bo < 2; ++bo)
+            G[(ai + 2 * ao) + 4 * (bi + 2 * bo)] = U[(ao + 2 * bo) * 4 + (ai + 2 * bi)];
+    std::vector<cd> Uf, Vh;
+    std::vector<double> s;
+    small_svd(4, 4, G, Uf, s, Vh);
+    int k = 0;
+    while (k < 4 && s[k] > 1e-12) ++k;
+    if (k == 0) k = 1;
+    // A[k, a_in, a_out] = U[(a_in,a_out), k] sqrt(s_k); B[k, b_in, b_out] = sqrt(s_k) Vh[k, (b_in,b_out)]
+    std::vector<cd> A(k * 4), B(k * 4);
+    for (int c = 0; c < k; ++c) {
+      const double sq = std::sqrt(std::abs(s[c]));
+      for (int rw = 0; rw < 4; ++rw) {
+        A[c + k * rw] = Uf[rw + 4 * c] * sq;
+        B[c + k * rw] = sq * Vh[c + 4 * rw];
+      }
+    }
+    const auto path = shortest_path(edges, qa, qb);
+    if (path.size() < 2) throw HostError(-1, "two-qubit gate between disconnected or equal qubits");
+    for (size_t i = 0; i < path.size(); ++i) {
+      const int si = site_index(path[i]);
+      if (i == 0) {
+        attach(ops[si], {leg_toward(si, path[1])}, {k}, A);
+      } else if (i + 1 == path.size()) {
+        attach(ops[si], {leg_toward(si, path[i - 1])}, {k}, B);
+      } else {
+        int lm = leg_toward(si, path[i - 1]), lp = leg_toward(si, path[i + 1]);
+        std::vector<cd> X(k * k * 4, 0.0);
+        for (int x = 0; x < k; ++x)
+          for (int o = 0; o < 2; ++o) X[x + k * x + k * k * (o + 2 * o)] = 1.0;
+        std::vector<int> legs = {std::min(lm, lp), std::max(lm, lp)};
+        attach(ops[si], legs, {k, k}, X);
+      }
+    }
+  }
+  void append(const Instruction& in) {
+    const auto U = gate_matrix(in);
+    const int nq = qubit_count(in);
+    if (nq == 1) one_qubit((int)in.qubits[0].index, U);
+    else if (nq == 2) two_qubit((int)in.qubits[0].index, (int)in.qubits[1].index, U);
+    else throw HostError(-6, "three-qubit gates are not supported on the estimator path");
+  }
+};
+
+static Layer pack_layer(const LayerBuilder& lb) {
+  Layer L;
+  const size_t ne = lb.edges.size();
+  L.edge_rank.assign(ne, 1);
+  for (size_t si = 0; si < lb.sites.size(); ++si)
+    for (size_t k = 0; k < lb.bonds[si].size(); ++k) L.edge_rank[lb.bonds[si][k]] = lb.ops[si].shape[k];
+  int64_t off = 0;
+  for (size_t si = 0; si < lb.sites.size(); ++si) {
+    L.op_offset.push_back(off);
+    for (auto& v : lb.ops[si].data) { L.op_data.push_back(v.real()); L.op_data.push_back(v.imag()); }
+    off += (int64_t)lb.ops[si].data.size();
+  }
+  return L;
+}
+
+// QasmToTPO, barrier layering (qasmtotpo.h:743-767): a new layer at every
+// barrier except a final one.
+std::vector<Layer> qasm_tpo(const Program& p, const Edges& edges) {
+  LayerBuilder lb(edges);
+  std::vector<Layer> out;
+  for (size_t i = 0; i < p.instructions.size(); ++i) {
+    const auto& in = p.instructions[i];
+    if (in.op == Op::BARRIER) {
+      if (i + 1 == p.instructions.size()) break;
+      out.push_back(pack_layer(lb));
+      lb.reset();
+      continue;
+    }
+    lb.append(in);
+  }
+  out.push_back(pack_layer(lb));
+  return out;
+}
+
+// One Floquet step of apps/kicked_ising_lattice/circuit.h:14-229:
+// exp(-i dt Jz Z Z) on every edge, then exp(-i dt hz Z), then exp(-i dt hx X).
+// exp(-i th ZZ) = cos(th) I(x)I - i sin(th) Z(x)Z, split term by term with
+// the magnitude shared evenly between the two sites.
+Layer kicked_ising_tpo(const Edges& edges, double Jz, double hz, double hx, double dt) {
+  LayerBuilder lb(edges);
+  const double th = dt * Jz;
+  const cd I(0, 1);
+  std::vector<std::pair<std::vector<cd>, std::vector<cd>>> terms;  // (A, B) 2x2 matrices U[out][in]
+  const double c = std::cos(th), s = std::sin(th);
+  if (std::abs(c) > 1e-15) {
+    const double a = std::sqrt(std::abs(c));
+    terms.push_back({{a, 0, 0, a}, {c / a, 0, 0, c / a}});
+  }
+  if (std::abs(s) > 1e-15) {
+    const double a = std::sqrt(std::abs(s));
+    const cd b = -I * s / a;
+    terms.push_back({{a, 0, 0, -a}, {b, 0, 0, -b}});
+  }
+  const int k = (int)terms.size();
+  std::vector<cd> A(k * 4), B(k * 4);
+  for (int t = 0; t < k; ++t) {
+    const auto xa = one_qubit_x(terms[t].first), xb = one_qubit_x(terms[t].second);
+    for (int r = 0; r < 4; ++r) { A[t + k * r] = xa[r]; B[t + k * r] = xb[r]; }
+  }
+  for (size_t m = 0; m < edges.size(); ++m) {
+    const int sa = lb.site_index(edges[m].first), sb = lb.site_index(edges[m].second);
+    attach(lb.ops[sa], {lb.leg_toward(sa, edges[m].second)}, {k}, A);
+    attach(lb.ops[sb], {lb.leg_toward(sb, edges[m].first)}, {k}, B);
+  }
+  const std::vector<cd> Uz = {std::exp(-I * (dt * hz)), 0, 0, std::exp(I * (dt * hz))};
+  const std::vector<cd> Ux = {std::cos(dt * hx), -I * std::sin(dt * hx), -I * std::sin(dt * hx), std::cos(dt * hx)};
+  for (size_t si = 0; si < lb.sites.size(); ++si) attach(lb.ops[si], {}, {}, one_qubit_x(Uz));
+  for (size_t si = 0; si < lb.sites.size(); ++si) attach(lb.ops[si], {}, {}, one_qubit_x(Ux));
+  return pack_layer(lb);
+}
+
+// -------------------------------------------------------------- Pauli
+// load_sparse_pauli_op (sparse_pauli.h:52-97) on text; classification of
+// ClassifyOps (paulitotpo.h:99-153).
+static void trim(std::string& s) {
+  auto ns = [](unsigned char c) { return !std::isspace(c); };
+  auto b = std::find_if(s.begin(), s.end(), ns);
+  auto e = std::find_if(s.rbegin(), s.rend(), ns).base();
+  if (b < e) s.assign(b, e); else s.clear();
+}
+
+std::vector<PauliTerm> pauli_terms(const std::string& text, const Edges& edges, int64_t* n_dropped) {
+  std::vector<PauliTerm> out;
+  std::istringstream in(text);
+  std::string line;
+  size_t lineno = 0;
+  int64_t row = 0, dropped = 0;
+  while (std::getline(in, line)) {
+    ++lineno;
+    trim(line);
+    if (line.empty() || line.rfind("#", 0) == 0 || line.rfind("//", 0) == 0) continue;
+    double re = 0, im = 0;
+    std::string ps;
+    std::istringstream a(line);
+    if (!(a >> re >> im >> ps)) {
+      std::istringstream b(line);
+      im = 0;
+      if (!(b >> re >> ps)) throw HostError(-5, "Parse error at line " + std::to_string(lineno) + ": \"" + line + "\"");
+    }
+    trim(ps);
+    for (char& ch : ps) {
+      ch = (char)std::toupper((unsigned char)ch);
+      if (ch != 'I' && ch != 'X' && ch != 'Y' && ch != 'Z')
+        throw HostError(-5, "Invalid Pauli label: only I/X/Y/Z are allowed.");
+    }
+    // rightmost character is qubit 0; keep non-identity letters, ascending qubit
+    std::vector<std::pair<int, char>> ops;
+    const size_t n = ps.size();
+    for (size_t i = 0; i < n; ++i) {
+      const char u = ps[n - 1 - i];
+      if (u != 'I') ops.push_back({(int)i, u});
+    }
+    PauliTerm t;
+    t.coeff_re = re;
+    t.coeff_im = im;
+    t.row = row++;
+    if (ops.size() == 1) {
+      t.kind = 1; t.q0 = ops[0].first; t.q1 = -1; t.l0 = ops[0].second; t.l1 = 0;
+      out.push_back(t);
+    } else if (ops.size() == 2) {
+      bool adj = false;
+      for (int m : surrounding_bonds(edges, ops[0].first)) {
+        const auto& e = edges[m];
+        if ((e.first == ops[0].first && e.second == ops[1].first) || (e.first == ops[1].first && e.second == ops[0].first)) { adj = true; break; }
+      }
+      if (adj) {
+        t.kind = 2; t.q0 = ops[0].first; t.q1 = ops[1].first; t.l0 = ops[0].second; t.l1 = ops[1].second;
+        out.push_back(t);
+      } else {
+        ++dropped;
+      }
+    } else {
+      ++dropped;
+    }
+  }
+  if (n_dropped) *n_dropped = dropped;
+  return out;
+}
+
+// PauliOpMatrix (paulitotpo.h:21-35) in the reference's tensor layout
+// O[c0, c1] = list[c0 + 2 c1].
+std::vector<cd> pauli_list(char l) {
+  const cd I(0, 1);
+  switch (l) {
+    case 'I': return {1, 0, 0, 1};
+    case 'X': return {0, 1, 1, 0};
+    case 'Y': return {0, -I, I, 0};
+    case 'Z': return {1, 0, 0, -1};
+    default: throw HostError(-6, "matrix for this op not implemented");
+  }
+}
+
+}  // namespace tnbp_host

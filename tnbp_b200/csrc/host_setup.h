@@ -1,0 +1,54 @@
+// Host-side problem builders (lattice, QASM, Pauli, TPO); see host_setup.cpp.
+#pragma once
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace tnbp_host {
+
+struct HostError : std::runtime_error {
+  int code;
+  HostError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+using Edges = std::vector<std::pair<int, int>>;
+
+// Same enumerator order as qasm::Op (include/qasm/ir.h:13-16).
+enum class Op { U3, U2, U1, RX, RY, RZ, H, X, Y, Z, S, SDG, T, TDG, ID, CX, CZ, SWAP, RZZ, CCX, CSWAP,
+                MEASURE, BARRIER, RESET, CUSTOM };
+struct QArg { std::string reg; size_t index = 0; };
+struct Instruction { Op op = Op::ID; std::vector<double> params; std::vector<QArg> qubits; };
+struct Program { std::vector<Instruction> instructions; };
+
+struct Layer {
+  std::vector<int32_t> edge_rank;
+  std::vector<int64_t> op_offset;
+  std::vector<double> op_data;  // interleaved complex
+};
+
+struct PauliTerm {
+  int kind = 0;  // 1 or 2
+  int q0 = -1, q1 = -1;
+  char l0 = 0, l1 = 0;
+  double coeff_re = 0, coeff_im = 0;
+  int64_t row = 0;
+};
+
+Edges square_lattice(int Lx, int Ly);
+std::vector<int> greedy_layering(const Edges& e, int* nlayers);
+std::vector<int> surrounding_bonds(const Edges& e, int site);
+std::vector<int> site_labels(const Edges& e);
+std::vector<int> shortest_path(const Edges& e, int src, int dst);
+Program parse_qasm(const std::string& src);
+int qubit_count(const Instruction& in);
+Edges qasm_edges(const Program& p);
+std::vector<Layer> qasm_tpo(const Program& p, const Edges& edges);
+Layer kicked_ising_tpo(const Edges& edges, double Jz, double hz, double hx, double dt);
+std::vector<PauliTerm> pauli_terms(const std::string& text, const Edges& edges, int64_t* n_dropped);
+std::vector<std::complex<double>> pauli_list(char letter);
+
+}  // namespace tnbp_host

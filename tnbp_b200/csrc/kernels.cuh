@@ -1,0 +1,381 @@
+// Device kernels of the BP / truncation / measurement hot path.
+//
+// Every kernel takes a device array of task descriptors so that one launch
+// covers all sites (or edges, or messages) of a stage, whatever their bond
+// dimensions: uneven shapes share a launch.  Blocks find their task by a
+// binary search over the tasks' exclusive prefix of block counts.
+#pragma once
+#include <cstdint>
+#include "cplx.cuh"
+
+namespace tnbp {
+
+constexpr int kThreads = 256;
+constexpr int kRowTile = 32;   // rows of a leg-apply / Gram tile
+constexpr int kColTile = 32;   // output columns per inner chunk
+constexpr int kMaxLegs = 8;    // maximum site degree supported
+constexpr int kSvdMaxSweeps = 60;
+
+// ---------------------------------------------------------------------------
+// Leg contraction  out[l, k, r] = sum_j in[l, j, r] * mat[j, k]
+//   in : L x Din x R, out : L x Dout x R (column-major), mat : Din x Dout.
+// Rows q = l + L*r are tiled by 32; a block owns one row tile and loops over
+// the output columns in chunks of 32 with the input tile kept in shared
+// memory.  This is the absorption of a message (bp.h:137-152) and of a
+// truncation projector (truncation.h:175-185, 206-216).
+// ---------------------------------------------------------------------------
+struct LegTask {
+  const void* in;
+  void* out;
+  const void* mat;
+  long long L, R;
+  int Din, Dout;
+  long long block_begin;  // exclusive prefix of row tiles over tasks
+};
+
+__device__ __forceinline__ int find_task(const long long* begins, int n, long long b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (begins[mid] <= b) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_leg_apply(const LegTask* __restrict__ tasks,
+                                                        const long long* __restrict__ begins,
+                                                        int ntask, int max_din) {
+  using C = typename cvec<R>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ti = find_task(begins, ntask, blockIdx.x);
+  const LegTask tk = tasks[ti];
+  const long long tile = blockIdx.x - tk.block_begin;
+  const long long rows = tk.L * tk.R;
+  const long long q0 = tile * kRowTile;
+  const int Din = tk.Din, Dout = tk.Dout;
+  const int ldA = Din + 1;
+  C* As = reinterpret_cast<C*>(smem_raw);              // [32][Din+1]
+  C* Ms = As + kRowTile * (max_din + 1);               // [Din][33]
+  const C* in = static_cast<const C*>(tk.in);
+  C* out = static_cast<C*>(tk.out);
+  const C* mat = static_cast<const C*>(tk.mat);
+  const long long L = tk.L;
+  const bool qfast = L >= kRowTile;
+
+  // input tile
+  const int nA = kRowTile * Din;
+  for (int idx = threadIdx.x; idx < nA; idx += kThreads) {
+    int qq, j;
+    if (qfast) { qq = idx % kRowTile; j = idx / kRowTile; }
+    else { j = idx % Din; qq = idx / Din; }
+    const long long q = q0 + qq;
+    C v = czero<C>();
+    if (q < rows) {
+      const long long l = q % L, r = q / L;
+      v = in[l + L * j + L * Din * r];
+    }
+    As[qq * ldA + j] = v;
+  }
+  for (int k0 = 0; k0 < Dout; k0 += kColTile) {
+    const int kc = min(kColTile, Dout - k0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < Din * kColTile; idx += kThreads) {
+      const int kk = idx % kColTile, j = idx / kColTile;
+      Ms[j * (kColTile + 1) + kk] = kk < kc ? mat[j + (long long)Din * (k0 + kk)] : czero<C>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < (kRowTile * kColTile) / kThreads; ++i) {
+      const int o = threadIdx.x + i * kThreads;
+      int qq, kk;
+      if (qfast) { qq = o % kRowTile; kk = o / kRowTile; }
+      else { kk = o % kColTile; qq = o / kColTile; }
+      C acc = czero<C>();
+      const C* a = As + qq * ldA;
+      const C* m = Ms + kk;
+      for (int j = 0; j < Din; ++j) cfma(acc, a[j], m[j * (kColTile + 1)]);
+      const long long q = q0 + qq;
+      if (q < rows && kk < kc) {
+        const long long l = q % L, r = q / L;
+        out[l + L * (k0 + kk) + L * (long long)Dout * r] = acc;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Gram with up to two kept legs:
+//   N[c, c'] = sum_q A[q, c] * conj(B[q, c'])
+// with q = l + L*m (l < L, m < M) and c = t + D*p (t < D, p < P) at address
+// l + L*t + L*D*m + L*D*M*p.  P = 1 gives the message contraction of
+// bp.h:157-166 (one kept leg); P = d gives the (d,d,D,D) environments of
+// measure.h:194-205 (kept target leg and physical leg).
+// Split-K: block = (row chunk, 32x32 tile of N); partial sums are written in
+// FP64 and reduced in a fixed order by k_msg_finalize (no float atomics).
+// ---------------------------------------------------------------------------
+struct GramTask {
+  const void* A;
+  const void* B;
+  long long L, M;
+  int D, P, C, ctiles;
+  long long Q, chunk_rows;
+  int nchunk;
+  double2* partial;       // [nchunk][C*C], N[c + C*c']
+  long long block_begin;  // exclusive prefix of nchunk*ctiles*ctiles
+};
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_gram(const GramTask* __restrict__ tasks,
+                                                   const long long* __restrict__ begins, int ntask) {
+  using C = typename cvec<R>::type;
+  __shared__ C As[kRowTile][kColTile + 1];
+  __shared__ C Bs[kRowTile][kColTile + 1];
+  const int ti = find_task(begins, ntask, blockIdx.x);
+  const GramTask tk = tasks[ti];
+  long long b = blockIdx.x - tk.block_begin;
+  const int tiles2 = tk.ctiles * tk.ctiles;
+  const int chunk = (int)(b / tiles2);
+  const int tt = (int)(b % tiles2);
+  const int ca0 = (tt % tk.ctiles) * kColTile;
+  const int cb0 = (tt / tk.ctiles) * kColTile;
+  const long long qbeg = chunk * tk.chunk_rows;
+  const long long qend = min(tk.Q, qbeg + tk.chunk_rows);
+  const C* A = static_cast<const C*>(tk.A);
+  const C* B = static_cast<const C*>(tk.B);
+  const long long L = tk.L, LD = tk.L * tk.D, LDM = tk.L * tk.D * tk.M;
+  const bool qfast = L >= kRowTile;
+  C acc[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) acc[i] = czero<C>();
+  for (long long q0 = qbeg; q0 < qend; q0 += kRowTile) {
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kRowTile * kColTile; idx += kThreads) {
+      int qq, cc;
+      if (qfast) { qq = idx % kRowTile; cc = idx / kRowTile; }
+      else { cc = idx % kColTile; qq = idx / kColTile; }
+      const long long q = q0 + qq;
+      C va = czero<C>(), vb = czero<C>();
+      if (q < qend) {
+        const long long l = q % L, m = q / L;
+        const long long base = l + LD * m;
+        const int c1 = ca0 + cc, c2 = cb0 + cc;
+        if (c1 < tk.C) va = A[base + L * (c1 % tk.D) + LDM * (c1 / tk.D)];
+        if (c2 < tk.C) vb = B[base + L * (c2 % tk.D) + LDM * (c2 / tk.D)];
+      }
+      As[qq][cc] = va;
+      Bs[qq][cc] = vb;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int o = threadIdx.x + i * kThreads;
+      const int a = o % kColTile, bb = o / kColTile;
+#pragma unroll 8
+      for (int qq = 0; qq < kRowTile; ++qq) cfma_conj(acc[i], As[qq][a], Bs[qq][bb]);
+    }
+  }
+  double2* part = tk.partial + (long long)chunk * tk.C * tk.C;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int o = threadIdx.x + i * kThreads;
+    const int a = ca0 + o % kColTile, bb = cb0 + o / kColTile;
+    if (a < tk.C && bb < tk.C) part[a + (long long)tk.C * bb] = to_d2(acc[i]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Reduce Gram partials (fixed order), normalize by the Frobenius norm
+// (bp.h:166), store the new message, and the distance to the normalized
+// stored message (bp.h:341-350).  One block per message.
+// ---------------------------------------------------------------------------
+struct MsgTask {
+  const double2* partial;
+  int nchunk, C;
+  void* out;        // new message (C x C), storage precision
+  const void* old;  // stored message (same dim) or nullptr
+  double* dist;     // || new/|new| - old/|old| ||_F
+  double* norm_out; // |N| before normalization (may be nullptr)
+};
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x < 32) {
+    t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) red[0] = t;
+  }
+  __syncthreads();
+  return red[0];
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_msg_finalize(const MsgTask* __restrict__ tasks) {
+  using C = typename cvec<R>::type;
+  __shared__ double red[32];
+  const MsgTask tk = tasks[blockIdx.x];
+  const int n = tk.C * tk.C;
+  const C* old = static_cast<const C*>(tk.old);
+  double s_new = 0.0, s_old = 0.0;
+  for (int i = threadIdx.x; i < n; i += kThreads) {
+    double2 v = make_double2(0.0, 0.0);
+    for (int c = 0; c < tk.nchunk; ++c) v = v + tk.partial[(long long)c * n + i];
+    s_new += abs2(v);
+    if (old) s_old += abs2(to_d2(old[i]));
+  }
+  const double nn = sqrt(block_sum(s_new, red));
+  const double no = old ? sqrt(block_sum(s_old, red)) : 0.0;
+  const double inv_n = nn > 0.0 ? 1.0 / nn : 1.0;
+  const double inv_o = no > 0.0 ? 1.0 / no : 1.0;
+  double d2 = 0.0;
+  C* out = static_cast<C*>(tk.out);
+  for (int i = threadIdx.x; i < n; i += kThreads) {
+    double2 v = make_double2(0.0, 0.0);
+    for (int c = 0; c < tk.nchunk; ++c) v = v + tk.partial[(long long)c * n + i];
+    v = inv_n * v;
+    if (old) d2 += abs2(v - inv_o * to_d2(old[i]));
+    out[i] = from_d2<C>(v);
+  }
+  d2 = block_sum(d2, red);
+  if (threadIdx.x == 0) {
+    if (tk.dist) *tk.dist = sqrt(d2);
+    if (tk.norm_out) *tk.norm_out = nn;
+  }
+}
+
+// cond = scale * sum_i x[i], fixed-order tree (one block).
+__global__ void k_sum_scaled(const double* __restrict__ x, int n, double scale, double* out) {
+  __shared__ double red[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += x[i];
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) *out = s * scale;
+}
+
+// ---------------------------------------------------------------------------
+// AbsorbTPO, site part (apply.h:43-66):
+//   V'[(v_0,o_0),...,(v_{g-1},o_{g-1}), p'] = sum_p O[o..., p, p'] V[v..., p]
+// merged bond index v + D*o (column-major reshape of (v, o)).
+// ---------------------------------------------------------------------------
+struct AbsorbTask {
+  const void* V;
+  void* out;
+  const double2* O;  // op tensor (r_0..r_{g-1}, d, d'), complex128
+  int g, d, dout;
+  int Dv[kMaxLegs];
+  int r[kMaxLegs];
+  long long n_out;
+  long long block_begin;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_absorb_sites(const AbsorbTask* __restrict__ tasks,
+                                                           const long long* __restrict__ begins,
+                                                           int ntask) {
+  using C = typename cvec<R>::type;
+  const int ti = find_task(begins, ntask, blockIdx.x);
+  const AbsorbTask& tk = tasks[ti];
+  const long long i = (blockIdx.x - tk.block_begin) * kThreads + threadIdx.x;
+  if (i >= tk.n_out) return;
+  long long rem = i;
+  long long voff = 0, vstride = 1, ooff = 0, ostride = 1;
+  for (int k = 0; k < tk.g; ++k) {
+    const long long M = (long long)tk.Dv[k] * tk.r[k];
+    const long long mk = rem % M;
+    rem /= M;
+    voff += (mk % tk.Dv[k]) * vstride;
+    ooff += (mk / tk.Dv[k]) * ostride;
+    vstride *= tk.Dv[k];
+    ostride *= tk.r[k];
+  }
+  const long long pout = rem;  // < dout
+  const C* V = static_cast<const C*>(tk.V);
+  double2 acc = make_double2(0.0, 0.0);
+  for (int p = 0; p < tk.d; ++p) {
+    const double2 v = to_d2(V[voff + vstride * p]);
+    const double2 o = tk.O[ooff + ostride * (p + (long long)tk.d * pout)];
+    acc = acc + v * o;
+  }
+  static_cast<C*>(tk.out)[i] = from_d2<C>(acc);
+}
+
+// AbsorbTPO, message part (apply.h:110-128): E'[(e,i),(e',i')] = E[e,e'] d_ii'.
+struct MsgExpandTask {
+  const void* E;
+  void* out;
+  int D, r;
+  long long block_begin;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_expand_msgs(const MsgExpandTask* __restrict__ tasks,
+                                                          const long long* __restrict__ begins,
+                                                          int ntask) {
+  using C = typename cvec<R>::type;
+  const int ti = find_task(begins, ntask, blockIdx.x);
+  const MsgExpandTask& tk = tasks[ti];
+  const long long N = (long long)tk.D * tk.r;
+  const long long i = (blockIdx.x - tk.block_begin) * kThreads + threadIdx.x;
+  if (i >= N * N) return;
+  const long long row = i % N, col = i / N;
+  const int e = (int)(row % tk.D), ii = (int)(row / tk.D);
+  const int e2 = (int)(col % tk.D), i2 = (int)(col / tk.D);
+  const C* E = static_cast<const C*>(tk.E);
+  static_cast<C*>(tk.out)[i] = (ii == i2) ? E[e + (long long)tk.D * e2] : czero<C>();
+}
+
+// ---------------------------------------------------------------------------
+// Sum of squares per range (site norms, tci::normalize on V), two passes:
+// k_sumsq_partial writes one double per block; k_scale_ranges has every block
+// re-add its range's partials in the same order and scale its elements.
+// ---------------------------------------------------------------------------
+struct RangeTask {
+  void* data;
+  long long n;
+  long long block_begin;
+  int nblocks;
+  double* partial;  // nblocks entries
+};
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_sumsq_partial(const RangeTask* __restrict__ tasks,
+                                                            const long long* __restrict__ begins,
+                                                            int ntask, int per_thread) {
+  using C = typename cvec<R>::type;
+  __shared__ double red[32];
+  const int ti = find_task(begins, ntask, blockIdx.x);
+  const RangeTask& tk = tasks[ti];
+  const long long b = blockIdx.x - tk.block_begin;
+  const long long beg = b * (long long)kThreads * per_thread;
+  const long long end = min(tk.n, beg + (long long)kThreads * per_thread);
+  const C* x = static_cast<const C*>(tk.data);
+  double s = 0.0;
+  for (long long i = beg + threadIdx.x; i < end; i += kThreads) s += abs2(to_d2(x[i]));
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) tk.partial[b] = s;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_scale_ranges(const RangeTask* __restrict__ tasks,
+                                                           const long long* __restrict__ begins,
+                                                           int ntask, int per_thread) {
+  using C = typename cvec<R>::type;
+  const int ti = find_task(begins, ntask, blockIdx.x);
+  const RangeTask& tk = tasks[ti];
+  double s = 0.0;
+  for (int i = 0; i < tk.nblocks; ++i) s += tk.partial[i];
+  const double nrm = sqrt(s);
+  const R inv = nrm > 0.0 ? (R)(1.0 / nrm) : (R)1;
+  const long long b = blockIdx.x - tk.block_begin;
+  const long long beg = b * (long long)kThreads * per_thread;
+  const long long end = min(tk.n, beg + (long long)kThreads * per_thread);
+  C* x = static_cast<C*>(tk.data);
+  for (long long i = beg + threadIdx.x; i < end; i += kThreads) x[i] = inv * x[i];
+}
+
+}  // namespace tnbp
