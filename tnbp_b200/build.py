@@ -1,6 +1,7 @@
 """Build libtnbp_b200.so in-tree for sm_100a with nvcc.
 
-Usage: python -m tnbp_b200.build  (or tnbp_b200.build.build()).
+Usage: python tnbp_b200/build.py (it does not import the package, which needs
+the built library).
 Objects are cached under tnbp_b200/_build/ and rebuilt when a source or
 header is newer than its object.
 """

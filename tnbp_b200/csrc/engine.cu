@@ -225,17 +225,40 @@ void* Job::vptr(int s) const { return static_cast<char*>(V.p) + voff[s] * esz; }
 void* Job::mptr(int arena, int m) const { return static_cast<char*>(M[arena].p) + moff[m] * esz; }
 
 void Job::destroy_graphs() {
-  for (int i = 0; i < 2; ++i) {
-    if (plan.graph_exec[i]) { cudaGraphExecDestroy(plan.graph_exec[i]); plan.graph_exec[i] = nullptr; }
+  plan.single[0].reset_graph();
+  plan.single[1].reset_graph();
+}
+
+void SweepBatch::reset_graph() {
+  if (graph) {
+    cudaGraphExecDestroy(graph);
+    graph = nullptr;
   }
+}
+SweepBatch& SweepBatch::operator=(SweepBatch&& o) noexcept {
+  if (this != &o) {
+    reset_graph();
+    levels = std::move(o.levels);
+    gram_tasks = std::move(o.gram_tasks);
+    gram_begins = std::move(o.gram_begins);
+    msg_tasks = std::move(o.msg_tasks);
+    sum_tasks = std::move(o.sum_tasks);
+    cond = std::move(o.cond);
+    gram_ntask = o.gram_ntask; nmsg = o.nmsg; nsum = o.nsum; gram_nblocks = o.gram_nblocks;
+    graph = o.graph;
+    o.graph = nullptr;
+  }
+  return *this;
+}
+uint64_t SweepBatch::bytes() const {
+  uint64_t b = gram_tasks.bytes + gram_begins.bytes + msg_tasks.bytes + sum_tasks.bytes + cond.bytes;
+  for (auto& l : levels) b += l.tasks.bytes + l.begins.bytes;
+  return b;
 }
 
 SweepPlan::~SweepPlan() {}
 uint64_t SweepPlan::bytes() const {
-  uint64_t b = scratch.bytes + partial.bytes + dist.bytes + cond.bytes + gram_tasks.bytes +
-               gram_begins.bytes + msg_tasks[0].bytes + msg_tasks[1].bytes;
-  for (auto& l : levels) b += l.tasks[0].bytes + l.tasks[1].bytes + l.begins.bytes;
-  return b;
+  return scratch.bytes + partial.bytes + dist.bytes + single[0].bytes() + single[1].bytes();
 }
 
 // --------------------------------------------------------------- sweep plan
@@ -320,49 +343,33 @@ void Job::build_plan() {
   };
   int maxlevel = 0;
   for (auto& op : ops) maxlevel = std::max(maxlevel, op.level + 1);
-  plan.levels.resize(maxlevel);
+  plan.levels.assign(maxlevel, LevelHost());
   plan.flops = 0.0;
   plan.bytes_alg = 0.0;
-  for (int lv = 0; lv < maxlevel; ++lv) {
-    std::vector<LegTask> t[2];
-    std::vector<long long> begins;
-    long long nb = 0;
-    int maxdin = 1;
-    for (auto& op : ops) {
-      if (op.level != lv) continue;
-      const auto sh = site_shape(op.site);
-      long long L = 1, R = 1;
-      for (int k = 0; k < op.leg; ++k) L *= sh[k];
-      for (size_t k = op.leg + 1; k < sh.size(); ++k) R *= sh[k];
-      const int D = sh[op.leg];
-      for (int par = 0; par < 2; ++par) {
-        LegTask lt;
-        lt.in = slot_ptr(op.site, op.src);
-        lt.out = slot_ptr(op.site, op.dst);
-        lt.mat = mptr(par, g.in_msg(op.site, op.leg));
-        lt.L = L; lt.R = R; lt.Din = D; lt.Dout = D;
-        lt.block_begin = nb;
-        t[par].push_back(lt);
-      }
-      begins.push_back(nb);
-      nb += (L * R + kRowTile - 1) / kRowTile;
-      maxdin = std::max(maxdin, D);
+  for (auto& op : ops) {
+    const auto sh = site_shape(op.site);
+    long long L = 1, R = 1;
+    for (int k = 0; k < op.leg; ++k) L *= sh[k];
+    for (size_t k = op.leg + 1; k < sh.size(); ++k) R *= sh[k];
+    const int D = sh[op.leg];
+    auto& lvh = plan.levels[op.level];
+    for (int par = 0; par < 2; ++par) {
+      LegTask lt;
+      lt.in = slot_ptr(op.site, op.src);
+      lt.out = slot_ptr(op.site, op.dst);
+      lt.mat = mptr(par, g.in_msg(op.site, op.leg));
+      lt.L = L; lt.R = R; lt.Din = D; lt.Dout = D;
+      lt.block_begin = 0;  // assigned when a batch is built
+      lvh.tasks[par].push_back(lt);
     }
-    upload_vec(plan.levels[lv].tasks[0], t[0], stream);
-    upload_vec(plan.levels[lv].tasks[1], t[1], stream);
-    upload_vec(plan.levels[lv].begins, begins, stream);
-    plan.levels[lv].ntask = (int)t[0].size();
-    plan.levels[lv].nblocks = nb;
-    plan.levels[lv].max_din = maxdin;
+    lvh.max_din = std::max(lvh.max_din, D);
   }
   // Gram + finalize tasks, one per directed message
-  std::vector<GramTask> gt;
-  std::vector<long long> gbeg;
-  std::vector<MsgTask> mt[2];
-  long long nb = 0;
   size_t part_elems = 0;
-  struct Pending { int s, t; size_t part_off; int nchunk, C; };
+  struct Pending { int s, t; size_t part_off; };
   std::vector<Pending> pend;
+  plan.gram.clear();
+  plan.gram_blocks.clear();
   for (int s = 0; s < ns; ++s) {
     const auto sh = site_shape(s);
     const int gs = (int)g.legs[s].size();
@@ -371,7 +378,7 @@ void Job::build_plan() {
     for (int k = 0; k < gs; ++k) sumD += sh[k];
     // algorithmic work of bp.h's schedule: 8 d prod(D) sum(D) flops per message
     plan.flops += gs * 8.0 * n * sumD;
-    plan.bytes_alg += n * esz + 2.0 * gs * 0.0;
+    plan.bytes_alg += n * esz;  // each site tensor read once
     for (int t = 0; t < gs; ++t) {
       GramTask g1;
       g1.A = slot_ptr(s, result[s][t]);
@@ -387,100 +394,186 @@ void Job::build_plan() {
       g1.chunk_rows = cr;
       g1.nchunk = (int)((g1.Q + cr - 1) / cr);
       g1.partial = nullptr;
-      g1.block_begin = nb;
-      gbeg.push_back(nb);
-      nb += (long long)g1.nchunk * g1.ctiles * g1.ctiles;
-      pend.push_back({s, t, part_elems, g1.nchunk, g1.C});
+      g1.block_begin = 0;
+      pend.push_back({s, t, part_elems});
       part_elems += (size_t)g1.nchunk * g1.C * g1.C;
-      gt.push_back(g1);
+      plan.gram.push_back(g1);
+      plan.gram_blocks.push_back((long long)g1.nchunk * g1.ctiles * g1.ctiles);
       plan.bytes_alg += 2.0 * sh[t] * sh[t] * esz;  // message in + out
     }
   }
   plan.partial.alloc(std::max<size_t>(part_elems, 1) * sizeof(double2), stream);
   plan.dist.alloc(std::max<size_t>(2 * ne, 1) * sizeof(double), stream);
-  plan.cond.alloc(sizeof(double) * 4, stream);
   double2* part = static_cast<double2*>(plan.partial.p);
-  for (size_t i = 0; i < gt.size(); ++i) {
-    gt[i].partial = part + pend[i].part_off;
+  plan.msg[0].clear();
+  plan.msg[1].clear();
+  for (size_t i = 0; i < plan.gram.size(); ++i) {
+    plan.gram[i].partial = part + pend[i].part_off;
     const int mo = g.out_msg(pend[i].s, pend[i].t);
     for (int par = 0; par < 2; ++par) {
       MsgTask m;
-      m.partial = gt[i].partial;
-      m.nchunk = pend[i].nchunk;
-      m.C = pend[i].C;
+      m.partial = plan.gram[i].partial;
+      m.nchunk = plan.gram[i].nchunk;
+      m.C = plan.gram[i].C;
       m.out = mptr(1 - par, mo);
       m.old = mptr(par, mo);
       m.dist = static_cast<double*>(plan.dist.p) + mo;
       m.norm_out = nullptr;
-      mt[par].push_back(m);
+      plan.msg[par].push_back(m);
     }
   }
-  upload_vec(plan.gram_tasks, gt, stream);
-  upload_vec(plan.gram_begins, gbeg, stream);
-  upload_vec(plan.msg_tasks[0], mt[0], stream);
-  upload_vec(plan.msg_tasks[1], mt[1], stream);
-  plan.gram_ntask = (int)gt.size();
-  plan.gram_nblocks = nb;
-  plan.nmsg = (int)mt[0].size();
   plan.valid = true;
+  for (int par = 0; par < 2; ++par) build_batch({{this, par}}, plan.single[par], stream);
   CK(cudaStreamSynchronize(stream));
   check_budget();
 }
 
+// Concatenate the sweep tasks of several jobs (each at its own message
+// parity) into one set of launches; block offsets are re-based so uneven
+// jobs share every launch.
+void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStream_t stream) {
+  b.reset_graph();
+  size_t nlev = 0;
+  for (auto& e : entries) {
+    if (!e.job->plan.valid) e.job->build_plan();
+    nlev = std::max(nlev, e.job->plan.levels.size());
+  }
+  b.levels.resize(nlev);
+  for (size_t lv = 0; lv < nlev; ++lv) {
+    std::vector<LegTask> t;
+    std::vector<long long> beg;
+    long long nb = 0;
+    int maxdin = 1;
+    for (auto& e : entries) {
+      const auto& P = e.job->plan;
+      if (lv >= P.levels.size()) continue;
+      for (LegTask lt : P.levels[lv].tasks[e.parity]) {
+        lt.block_begin = nb;
+        beg.push_back(nb);
+        nb += (lt.L * lt.R + kRowTile - 1) / kRowTile;
+        t.push_back(lt);
+      }
+      maxdin = std::max(maxdin, P.levels[lv].max_din);
+    }
+    upload_vec(b.levels[lv].tasks, t, stream);
+    upload_vec(b.levels[lv].begins, beg, stream);
+    b.levels[lv].ntask = (int)t.size();
+    b.levels[lv].nblocks = nb;
+    b.levels[lv].max_din = maxdin;
+  }
+  std::vector<GramTask> gt;
+  std::vector<long long> gb;
+  std::vector<MsgTask> mt;
+  std::vector<SumTask> st;
+  long long nb = 0;
+  for (size_t ei = 0; ei < entries.size(); ++ei) {
+    const auto& P = entries[ei].job->plan;
+    for (size_t i = 0; i < P.gram.size(); ++i) {
+      GramTask g1 = P.gram[i];
+      g1.block_begin = nb;
+      gb.push_back(nb);
+      nb += P.gram_blocks[i];
+      gt.push_back(g1);
+    }
+    for (auto& m : P.msg[entries[ei].parity]) mt.push_back(m);
+    SumTask s1;
+    s1.x = static_cast<const double*>(P.dist.p);
+    s1.n = (int)P.msg[0].size();
+    s1.scale = 1.0 / (2.0 * (double)entries[ei].job->g.edges.size());
+    s1.out = nullptr;  // patched after cond is allocated
+    st.push_back(s1);
+  }
+  b.cond.alloc(std::max<size_t>(entries.size(), 1) * sizeof(double), stream);
+  for (size_t i = 0; i < st.size(); ++i) st[i].out = static_cast<double*>(b.cond.p) + i;
+  upload_vec(b.gram_tasks, gt, stream);
+  upload_vec(b.gram_begins, gb, stream);
+  upload_vec(b.msg_tasks, mt, stream);
+  upload_vec(b.sum_tasks, st, stream);
+  b.gram_ntask = (int)gt.size();
+  b.gram_nblocks = nb;
+  b.nmsg = (int)mt.size();
+  b.nsum = (int)st.size();
+}
+
 template <typename R>
-void Job::launch_sweep_kernels(int par) {
-  for (auto& lv : plan.levels) {
+static size_t leg_smem(int max_din) {
+  return (size_t)(kRowTile * (max_din + 1) + max_din * (kColTile + 1)) * sizeof(typename cvec<R>::type);
+}
+
+// Largest dynamic shared memory any leg-apply launch may ask for; set once
+// per process outside of stream capture.
+template <typename R>
+static void leg_apply_attr() {
+  static bool done = false;
+  if (done) return;
+  CK(cudaFuncSetAttribute(k_leg_apply<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)leg_smem<R>(128)));
+  done = true;
+}
+
+template <typename R>
+static void launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
+  for (auto& lv : b.levels) {
     if (lv.ntask == 0) continue;
-    const size_t smem = (size_t)(kRowTile * (lv.max_din + 1) + lv.max_din * (kColTile + 1)) * sizeof(typename cvec<R>::type);
-    CK(cudaFuncSetAttribute(k_leg_apply<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (lv.max_din > 128) throw Error(TNBP_EUNSUPPORTED, "bond dimension above 128 during BP");
+    const size_t smem = leg_smem<R>(lv.max_din);
     k_leg_apply<R><<<(unsigned)lv.nblocks, kThreads, smem, stream>>>(
-        static_cast<const LegTask*>(lv.tasks[par].p), static_cast<const long long*>(lv.begins.p), lv.ntask,
-        lv.max_din);
+        static_cast<const LegTask*>(lv.tasks.p), static_cast<const long long*>(lv.begins.p), lv.ntask, lv.max_din);
     CK(cudaGetLastError());
   }
-  k_gram<R><<<(unsigned)plan.gram_nblocks, kThreads, 0, stream>>>(
-      static_cast<const GramTask*>(plan.gram_tasks.p), static_cast<const long long*>(plan.gram_begins.p),
-      plan.gram_ntask);
-  CK(cudaGetLastError());
-  k_msg_finalize<R><<<plan.nmsg, kThreads, 0, stream>>>(static_cast<const MsgTask*>(plan.msg_tasks[par].p));
-  CK(cudaGetLastError());
-  k_sum_scaled<<<1, kThreads, 0, stream>>>(static_cast<const double*>(plan.dist.p), plan.nmsg,
-                                           1.0 / (2.0 * (double)g.edges.size()),
-                                           static_cast<double*>(plan.cond.p));
-  CK(cudaGetLastError());
+  if (b.gram_ntask) {
+    k_gram<R><<<(unsigned)b.gram_nblocks, kThreads, 0, stream>>>(
+        static_cast<const GramTask*>(b.gram_tasks.p), static_cast<const long long*>(b.gram_begins.p), b.gram_ntask);
+    CK(cudaGetLastError());
+    k_msg_finalize<R><<<b.nmsg, kThreads, 0, stream>>>(static_cast<const MsgTask*>(b.msg_tasks.p));
+    CK(cudaGetLastError());
+  }
+  if (b.nsum) {
+    k_segmented_sum<<<b.nsum, kThreads, 0, stream>>>(static_cast<const SumTask*>(b.sum_tasks.p));
+    CK(cudaGetLastError());
+  }
+}
+
+void launch_batch(const SweepBatch& b, int prec, cudaStream_t stream) {
+  if (prec == TNBP_C128) launch_batch_t<double>(b, stream);
+  else launch_batch_t<float>(b, stream);
+}
+
+void prepare_kernels(int prec) {
+  if (prec == TNBP_C128) leg_apply_attr<double>();
+  else leg_apply_attr<float>();
 }
 
 void Job::run_sweep(int par) {
   if (!plan.valid) build_plan();
-  if (!plan.graph_exec[par]) {
-    // warm the function attributes outside capture, then capture once
+  SweepBatch& b = plan.single[par];
+  if (!b.graph) {
+    prepare_kernels(prec);
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     try {
-      if (prec == TNBP_C128) launch_sweep_kernels<double>(par);
-      else launch_sweep_kernels<float>(par);
+      launch_batch(b, prec, stream);
     } catch (...) {
       cudaStreamEndCapture(stream, &graph);
       throw;
     }
     CK(cudaStreamEndCapture(stream, &graph));
-    CK(cudaGraphInstantiate(&plan.graph_exec[par], graph, 0));
+    CK(cudaGraphInstantiate(&b.graph, graph, 0));
     cudaGraphDestroy(graph);
   }
   CK(cudaEventRecord(ev0, stream));
-  CK(cudaGraphLaunch(plan.graph_exec[par], stream));
+  CK(cudaGraphLaunch(b.graph, stream));
   CK(cudaEventRecord(ev1, stream));
+  last_par = par;
   sweeps_run++;
 }
 
 double Job::read_cond() {
-  CK(cudaMemcpyAsync(host_scalar, plan.cond.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
+  CK(cudaMemcpyAsync(host_scalar, plan.single[last_par].cond.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) last_sweep_ms = ms;
   return host_scalar[0];
 }
-
 void Job::bp_sweep() {
   run_sweep(cur);
   cur = 1 - cur;
@@ -646,13 +739,13 @@ void Job::run_chains(std::vector<ChainEntry>& chains) {
     DevBuf dt, db;
     upload_vec(dt, t, stream);
     upload_vec(db, b, stream);
+    if (maxdin > 128) throw Error(TNBP_EUNSUPPORTED, "bond dimension above 128");
+    prepare_kernels(prec);
     if (prec == TNBP_C128) {
-      const size_t smem = (size_t)(kRowTile * (maxdin + 1) + maxdin * (kColTile + 1)) * 16;
-      CK(cudaFuncSetAttribute(k_leg_apply<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      const size_t smem = leg_smem<double>(maxdin);
       k_leg_apply<double><<<(unsigned)nb, kThreads, smem, stream>>>(static_cast<LegTask*>(dt.p), static_cast<long long*>(db.p), (int)t.size(), maxdin);
     } else {
-      const size_t smem = (size_t)(kRowTile * (maxdin + 1) + maxdin * (kColTile + 1)) * 8;
-      CK(cudaFuncSetAttribute(k_leg_apply<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      const size_t smem = leg_smem<float>(maxdin);
       k_leg_apply<float><<<(unsigned)nb, kThreads, smem, stream>>>(static_cast<LegTask*>(dt.p), static_cast<long long*>(db.p), (int)t.size(), maxdin);
     }
     CK(cudaGetLastError());

@@ -9,6 +9,8 @@
 #include <utility>
 #include <vector>
 
+#include "kernels.cuh"
+
 namespace tnbp {
 
 struct Error : std::runtime_error {
@@ -56,22 +58,39 @@ struct Graph {
   int in_msg(int s, int k) const;
 };
 
-struct LevelTasks {
-  DevBuf tasks[2];
-  DevBuf begins;
-  int ntask = 0;
-  long long nblocks = 0;
+struct LevelHost {
+  std::vector<LegTask> tasks[2];  // per message-arena parity
   int max_din = 1;
+};
+
+// Device task arrays of one sweep launch sequence; built from one job (the
+// per-job path, captured once per parity as a CUDA graph) or from many jobs
+// at once (the served path: every active job's sweep in the same launches).
+struct SweepBatch {
+  struct Level { DevBuf tasks, begins; int ntask = 0; long long nblocks = 0; int max_din = 1; };
+  std::vector<Level> levels;
+  DevBuf gram_tasks, gram_begins, msg_tasks, sum_tasks, cond;
+  int gram_ntask = 0, nmsg = 0, nsum = 0;
+  long long gram_nblocks = 0;
+  cudaGraphExec_t graph = nullptr;
+  SweepBatch() = default;
+  SweepBatch(const SweepBatch&) = delete;
+  SweepBatch& operator=(const SweepBatch&) = delete;
+  SweepBatch(SweepBatch&& o) noexcept { *this = std::move(o); }
+  SweepBatch& operator=(SweepBatch&& o) noexcept;
+  ~SweepBatch() { reset_graph(); }
+  void reset_graph();
+  uint64_t bytes() const;
 };
 
 struct SweepPlan {
   bool valid = false;
-  DevBuf scratch, partial, dist, cond;
-  std::vector<LevelTasks> levels;
-  DevBuf gram_tasks, gram_begins, msg_tasks[2];
-  int gram_ntask = 0, nmsg = 0;
-  long long gram_nblocks = 0;
-  cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+  DevBuf scratch, partial, dist;
+  std::vector<LevelHost> levels;
+  std::vector<GramTask> gram;
+  std::vector<long long> gram_blocks;  // blocks of each gram task
+  std::vector<MsgTask> msg[2];
+  SweepBatch single[2];
   double flops = 0.0, bytes_alg = 0.0;
   SweepPlan() = default;
   SweepPlan(SweepPlan&&) = default;
@@ -79,6 +98,12 @@ struct SweepPlan {
   ~SweepPlan();
   uint64_t bytes() const;
 };
+
+struct Job;
+struct BatchEntry { Job* job; int parity; };
+void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStream_t stream);
+void launch_batch(const SweepBatch& b, int prec, cudaStream_t stream);
+void prepare_kernels(int prec);
 
 // A TPO layer on the device: complex128 op tensors of shape
 // (r_leg0..r_leg{g-1}, d, d') per site.
@@ -115,6 +140,7 @@ struct Job {
   size_t v_elems = 0, m_elems = 0;
   DevBuf V, M[2];
   int cur = 0;
+  int last_par = 0;
   SweepPlan plan;
   long long sweeps_run = 0;
   float last_sweep_ms = 0.f;
@@ -132,7 +158,6 @@ struct Job {
   void* mptr(int arena, int m) const;
   void destroy_graphs();
   void build_plan();
-  template <typename R> void launch_sweep_kernels(int par);
   void run_sweep(int par);
   double read_cond();
   void bp_sweep();

@@ -248,8 +248,24 @@ __global__ void __launch_bounds__(kThreads) k_msg_finalize(const MsgTask* __rest
   }
 }
 
+// One block per job of a batch: out = scale * sum_i x[i] (fixed order).
+struct SumTask {
+  const double* x;
+  int n;
+  double scale;
+  double* out;
+};
+static __global__ void k_segmented_sum(const SumTask* __restrict__ tasks) {
+  __shared__ double red[32];
+  const SumTask tk = tasks[blockIdx.x];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < tk.n; i += blockDim.x) s += tk.x[i];
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) *tk.out = s * tk.scale;
+}
+
 // cond = scale * sum_i x[i], fixed-order tree (one block).
-__global__ void k_sum_scaled(const double* __restrict__ x, int n, double scale, double* out) {
+static __global__ void k_sum_scaled(const double* __restrict__ x, int n, double scale, double* out) {
   __shared__ double red[32];
   double s = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) s += x[i];

@@ -12,7 +12,7 @@ struct PartialSumTask {
   int n;
   double2* out;
 };
-__global__ void k_partial_sum(const PartialSumTask* __restrict__ tasks) {
+static __global__ void k_partial_sum(const PartialSumTask* __restrict__ tasks) {
   const PartialSumTask tk = tasks[blockIdx.x];
   for (int i = threadIdx.x; i < tk.n; i += blockDim.x) {
     double2 v = make_double2(0.0, 0.0);
@@ -36,7 +36,7 @@ struct TermTask {
   double2 coeff;
 };
 
-__global__ void __launch_bounds__(kThreads) k_terms(const TermTask* __restrict__ tasks,
+static __global__ void __launch_bounds__(kThreads) k_terms(const TermTask* __restrict__ tasks,
                                                     double2* __restrict__ values) {
   __shared__ double red[32];
   const TermTask& tk = tasks[blockIdx.x];
@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(kThreads) k_terms(const TermTask* __restrict__
 }
 
 // sum_k c_k <P_k> (FP64, one block, fixed order)
-__global__ void k_weighted_sum(const TermTask* __restrict__ tasks, const double2* __restrict__ values,
+static __global__ void k_weighted_sum(const TermTask* __restrict__ tasks, const double2* __restrict__ values,
                                int n, double2* out) {
   __shared__ double red[32];
   double sr = 0.0, si = 0.0;

@@ -1,2 +1,312 @@
-// Continuous-batching request loop; filled in below the engine.
+// Continuous-batching request loop (the served estimator path).
+//
+// Requests wait in a FIFO queue and are admitted while their estimated peak
+// HBM footprint fits the budget and a slot is free.  Each admitted request
+// owns a device-resident Job (site tensors, messages, sweep plan) for its
+// whole life.  Every server step:
+//   1. admits queued requests;
+//   2. absorbs the next TPO layer for requests entering a Floquet step;
+//   3. runs ONE batched BP sweep over all requests in their BP phase: the
+//      leg-contraction, Gram and message kernels each take the concatenated
+//      task lists of every such job (uneven lattices and bond dimensions share
+//      each launch), with one condition per job;
+//   4. truncates requests whose BP loop ended, and measures finished ones.
+// Requests that arrive while others are on the GPU join at the next step, so
+// their sweeps overlap with the sweeps already in flight.  The BP stopping
+// rule per job is the one of Job::bp_run (the apps' loop), so a request's
+// result does not depend on what it was batched with.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "../../include/tnbp_b200.h"
+#include "host_setup.h"
 #include "server.h"
+
+namespace tnbp {
+
+Server::Server(int precision, uint64_t budget_bytes, int max_active_jobs)
+    : prec(precision), budget(budget_bytes), max_active(max_active_jobs) {
+  if (precision != TNBP_C128 && precision != TNBP_C64) throw Error(TNBP_EINVAL, "unknown precision");
+  if (max_active < 1) throw Error(TNBP_EINVAL, "max_active must be >= 1");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    throw Error(TNBP_ENOGPU, "no CUDA device visible: the B200 engine has no CPU path");
+  }
+  CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  if (budget == 0) {
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    const size_t reserve = (size_t)4 << 30;
+    budget = fr > 2 * reserve ? fr - reserve : fr / 2;
+  }
+}
+
+Server::~Server() {
+  batch = SweepBatch();
+  for (auto& kv : reqs) { kv.second->job.reset(); kv.second->tpo.reset(); }
+  if (hcond) cudaFreeHost(hcond);
+  if (stream) { cudaStreamSynchronize(stream); cudaStreamDestroy(stream); }
+}
+
+// Peak device bytes of a kicked-Ising request on an L x L lattice: BP runs
+// at bond dimension 2*chi; per site the tensor, its copy during absorption
+// and truncation, and the sweep scratch slots of its degree; both message
+// arenas twice; per-edge truncation work.
+uint64_t Server::footprint(const Request& r) const {
+  const double esz = prec == TNBP_C128 ? 16.0 : 8.0;
+  const double D = 2.0 * r.chi;
+  const int L = r.L;
+  double bytes = 0.0;
+  for (int y = 0; y < L; ++y)
+    for (int x = 0; x < L; ++x) {
+      const int g = (x > 0) + (x < L - 1) + (y > 0) + (y < L - 1);
+      const int slots = g == 4 ? 8 : g == 3 ? 5 : g == 2 ? 2 : 0;
+      const double n = 2.0 * std::pow(D, g);
+      bytes += n * esz * (2.0 + slots);
+    }
+  const double ne = 2.0 * L * (L - 1);
+  bytes += 4.0 * 2.0 * ne * D * D * esz;      // message arenas (old + new)
+  bytes += ne * 8.0 * D * D * 16.0;           // truncation work
+  bytes += 2.0 * ne * 16.0 * D * D * 16.0;    // Gram partials (upper bound)
+  return (uint64_t)(bytes * 1.1) + (8ull << 20);
+}
+
+int64_t Server::submit(std::unique_ptr<Request> r) {
+  if (r->L < 2) throw Error(TNBP_EINVAL, "lattice side must be >= 2");
+  if (r->chi < 1 || r->steps < 0 || r->maxit < 0) throw Error(TNBP_EINVAL, "bad request parameters");
+  r->footprint = footprint(*r);
+  if (r->footprint > budget) throw Error(TNBP_ENOMEM, "request footprint exceeds the server's HBM budget");
+  r->id = next_id++;
+  const int64_t id = r->id;
+  queue.push_back(id);
+  reqs[id] = std::move(r);
+  return id;
+}
+
+void Server::start(Request& r) {
+  const auto edges = tnbp_host::square_lattice(r.L, r.L);
+  std::vector<int32_t> e(2 * edges.size());
+  for (size_t i = 0; i < edges.size(); ++i) { e[2 * i] = edges[i].first; e[2 * i + 1] = edges[i].second; }
+  r.job = std::make_unique<Job>(e.data(), (int64_t)edges.size(), nullptr, prec, stream, 0);
+  // RZZ(theta_j) = exp(-i theta_j/2 ZZ), RX(theta_h) = exp(-i theta_h/2 X)
+  const auto layer = tnbp_host::kicked_ising_tpo(edges, r.theta_j / 2.0, 0.0, r.theta_h / 2.0, 1.0);
+  auto t = std::make_unique<Tpo>();
+  t->rank.assign(layer.edge_rank.begin(), layer.edge_rank.end());
+  t->op_offset = layer.op_offset;
+  t->dout.assign(r.job->g.labels.size(), 2);
+  t->ops.alloc(layer.op_data.size() * sizeof(double), stream);
+  CK(cudaMemcpyAsync(t->ops.p, layer.op_data.data(), layer.op_data.size() * sizeof(double), cudaMemcpyHostToDevice,
+                     stream));
+  CK(cudaStreamSynchronize(stream));
+  r.tpo = std::move(t);
+  r.step = 0;
+  r.phase = r.steps > 0 ? Request::ABSORB : Request::MEASURE;
+}
+
+void Server::finish(Request& r) {
+  std::vector<TermSpec> terms(r.kind.size());
+  for (size_t i = 0; i < r.kind.size(); ++i) {
+    TermSpec& t = terms[i];
+    std::memset(&t, 0, sizeof(t));
+    t.kind = r.kind[i];
+    t.coeff[0] = r.coeff[2 * i];
+    t.coeff[1] = r.coeff[2 * i + 1];
+    if (t.kind == 1) {
+      auto it = r.job->g.index_of.find(r.q0[i]);
+      if (it == r.job->g.index_of.end()) throw Error(TNBP_EINVAL, "term on a qubit outside the lattice");
+      t.site_a = it->second;
+      auto P = tnbp_host::pauli_list(r.letters[2 * i]);
+      for (int k = 0; k < 4; ++k) { t.op[2 * k] = P[k].real(); t.op[2 * k + 1] = P[k].imag(); }
+    } else {
+      t.edge = r.job->edge_of(r.q0[i], r.q1[i]);
+      if (t.edge < 0) throw Error(TNBP_EINVAL, "two-site term on a non-adjacent pair");
+      t.label_a = r.q0[i];
+      auto Pa = tnbp_host::pauli_list(r.letters[2 * i]);
+      auto Pb = tnbp_host::pauli_list(r.letters[2 * i + 1]);
+      for (int i0 = 0; i0 < 2; ++i0)
+        for (int i1 = 0; i1 < 2; ++i1)
+          for (int i2 = 0; i2 < 2; ++i2)
+            for (int i3 = 0; i3 < 2; ++i3) {
+              const auto v = Pa[i0 + 2 * i2] * Pb[i1 + 2 * i3];
+              const int idx = i0 + 2 * i1 + 4 * i2 + 8 * i3;
+              t.op[2 * idx] = v.real();
+              t.op[2 * idx + 1] = v.imag();
+            }
+    }
+  }
+  r.job->measure_terms(terms, nullptr, r.result);
+  r.job.reset();
+  r.tpo.reset();
+  r.phase = Request::DONE;
+}
+
+void Server::step(int* n_active, int* n_queued, int* n_done) {
+  int done = 0;
+  // 1. admission by HBM footprint and free slots
+  while (!queue.empty() && (int)active.size() < max_active) {
+    Request& r = *reqs[queue.front()];
+    if (!active.empty() && in_use + r.footprint > budget) break;
+    queue.pop_front();
+    start(r);
+    in_use += r.footprint;
+    active.push_back(r.id);
+  }
+  // 2. TPO absorption for requests entering a Floquet step
+  for (int64_t id : active) {
+    Request& r = *reqs[id];
+    if (r.phase == Request::ABSORB) {
+      r.job->absorb_tpo(*r.tpo);
+      r.phase = Request::BP;
+      r.bp_iters = 0;
+      if (r.maxit <= 0) r.phase = Request::TRUNC;
+    }
+  }
+  // 3. one batched BP sweep over every request in its BP phase
+  std::vector<BatchEntry> entries;
+  std::vector<Request*> inbp;
+  for (int64_t id : active) {
+    Request& r = *reqs[id];
+    if (r.phase == Request::BP) {
+      entries.push_back({r.job.get(), r.job->cur});
+      inbp.push_back(&r);
+    }
+  }
+  if (!entries.empty()) {
+    for (auto* r : inbp) if (!r->job->plan.valid) r->job->build_plan();
+    prepare_kernels(prec);
+    build_batch(entries, batch, stream);
+    launch_batch(batch, prec, stream);
+    if (hcond_cap < entries.size()) {
+      if (hcond) cudaFreeHost(hcond);
+      hcond_cap = std::max<size_t>(64, 2 * entries.size());
+      CK(cudaMallocHost(&hcond, hcond_cap * sizeof(double)));
+    }
+    CK(cudaMemcpyAsync(hcond, batch.cond.p, entries.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    for (size_t i = 0; i < inbp.size(); ++i) {
+      Request& r = *inbp[i];
+      Job& j = *r.job;
+      if (r.bp_iters == 0) {  // first sweep of the loop: always kept
+        j.cur = 1 - j.cur;
+        r.bp_iters = 1;
+        continue;
+      }
+      const double c = hcond[i];
+      if (c < r.tol || r.bp_iters >= r.maxit) {
+        r.phase = Request::TRUNC;  // keep the current messages
+      } else {
+        j.cur = 1 - j.cur;
+        ++r.bp_iters;
+      }
+    }
+  }
+  // 4. truncation, next step or measurement
+  for (int64_t id : active) {
+    Request& r = *reqs[id];
+    if (r.phase == Request::TRUNC) {
+      r.job->truncate(r.chi, r.sv_min, nullptr, nullptr);
+      ++r.step;
+      r.phase = r.step < r.steps ? Request::ABSORB : Request::MEASURE;
+    }
+    if (r.phase == Request::MEASURE) {
+      finish(r);
+      in_use -= r.footprint;
+      ++done;
+    }
+  }
+  active.erase(std::remove_if(active.begin(), active.end(),
+                              [&](int64_t id) { return reqs[id]->phase == Request::DONE; }),
+               active.end());
+  if (n_active) *n_active = (int)active.size();
+  if (n_queued) *n_queued = (int)queue.size();
+  if (n_done) *n_done = done;
+}
+
+}  // namespace tnbp
+
+// ------------------------------------------------------------------ C ABI
+struct tnbp_server { std::unique_ptr<tnbp::Server> s; };
+
+namespace {
+template <class F>
+int sguard(F&& f) {
+  try {
+    tnbp::g_last_error.clear();
+    f();
+    return TNBP_OK;
+  } catch (const tnbp::Error& e) {
+    tnbp::g_last_error = e.what();
+    return e.code;
+  } catch (const tnbp_host::HostError& e) {
+    tnbp::g_last_error = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    tnbp::g_last_error = e.what();
+    return TNBP_EINVAL;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int tnbp_server_create(int32_t precision, uint64_t budget, int32_t max_active, tnbp_server** out) {
+  return sguard([&] {
+    if (!out) throw tnbp::Error(TNBP_EINVAL, "out is NULL");
+    *out = nullptr;
+    auto s = std::make_unique<tnbp_server>();
+    s->s = std::make_unique<tnbp::Server>(precision, budget, max_active);
+    *out = s.release();
+  });
+}
+
+int tnbp_server_destroy(tnbp_server* srv) { return sguard([&] { delete srv; }); }
+
+int tnbp_server_submit_kicked_ising(tnbp_server* srv, int32_t L, int32_t chi, int32_t n_steps, double theta_j,
+                                    double theta_h, double bp_tol, int32_t bp_max_iter, double sv_min,
+                                    int64_t n_terms, const int32_t* kind, const int32_t* q0, const int32_t* q1,
+                                    const char* letters, const double* coeff, int64_t* request_id) {
+  return sguard([&] {
+    if (!srv) throw tnbp::Error(TNBP_EINVAL, "server is NULL");
+    if (n_terms > 0 && !(kind && q0 && q1 && letters && coeff)) throw tnbp::Error(TNBP_EINVAL, "NULL term arrays");
+    auto r = std::make_unique<tnbp::Request>();
+    r->L = L; r->chi = chi; r->steps = n_steps; r->theta_j = theta_j; r->theta_h = theta_h;
+    r->tol = bp_tol; r->maxit = bp_max_iter; r->sv_min = sv_min;
+    r->kind.assign(kind, kind + n_terms);
+    r->q0.assign(q0, q0 + n_terms);
+    r->q1.assign(q1, q1 + n_terms);
+    r->letters.assign(letters, letters + 2 * n_terms);
+    r->coeff.assign(coeff, coeff + 2 * n_terms);
+    for (int64_t i = 0; i < n_terms; ++i)
+      if (r->kind[i] != 1 && r->kind[i] != 2) throw tnbp::Error(TNBP_EINVAL, "term kind must be 1 or 2");
+    const int64_t id = srv->s->submit(std::move(r));
+    if (request_id) *request_id = id;
+  });
+}
+
+int tnbp_server_step(tnbp_server* srv, int32_t* n_active, int32_t* n_queued, int32_t* n_done) {
+  return sguard([&] {
+    if (!srv) throw tnbp::Error(TNBP_EINVAL, "server is NULL");
+    int a = 0, q = 0, d = 0;
+    srv->s->step(&a, &q, &d);
+    if (n_active) *n_active = a;
+    if (n_queued) *n_queued = q;
+    if (n_done) *n_done = d;
+  });
+}
+
+int tnbp_server_result(tnbp_server* srv, int64_t id, double* sum, int32_t* pending) {
+  return sguard([&] {
+    if (!srv) throw tnbp::Error(TNBP_EINVAL, "server is NULL");
+    auto it = srv->s->reqs.find(id);
+    if (it == srv->s->reqs.end()) throw tnbp::Error(TNBP_EINVAL, "unknown request id");
+    const bool done = it->second->phase == tnbp::Request::DONE;
+    if (pending) *pending = done ? 0 : 1;
+    if (sum && done) { sum[0] = it->second->result[0]; sum[1] = it->second->result[1]; }
+  });
+}
+
+}  // extern "C"

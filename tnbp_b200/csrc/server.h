@@ -1,2 +1,55 @@
-// Continuous-batching request loop (see server.cu).
+// Continuous-batching request loop over device-resident estimator jobs.
 #pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+namespace tnbp {
+
+struct Request {
+  enum Phase { QUEUED, ABSORB, BP, TRUNC, MEASURE, DONE };
+  int64_t id = 0;
+  int L = 0, chi = 0, steps = 0, maxit = 0;
+  double theta_j = 0, theta_h = 0, tol = 0, sv_min = 0;
+  std::vector<int32_t> kind, q0, q1;
+  std::string letters;
+  std::vector<double> coeff;
+  Phase phase = QUEUED;
+  std::unique_ptr<Job> job;
+  std::unique_ptr<Tpo> tpo;
+  int step = 0, bp_iters = 0;
+  uint64_t footprint = 0;
+  double result[2] = {0, 0};
+};
+
+struct Server {
+  int prec;
+  uint64_t budget;
+  int max_active;
+  cudaStream_t stream = nullptr;
+  double* hcond = nullptr;
+  size_t hcond_cap = 0;
+  int64_t next_id = 1;
+  std::deque<int64_t> queue;
+  std::map<int64_t, std::unique_ptr<Request>> reqs;
+  std::vector<int64_t> active;
+  uint64_t in_use = 0;
+  SweepBatch batch;
+
+  Server(int precision, uint64_t budget_bytes, int max_active_jobs);
+  ~Server();
+  int64_t submit(std::unique_ptr<Request> r);
+  void step(int* n_active, int* n_queued, int* n_done);
+  uint64_t footprint(const Request& r) const;
+  void start(Request& r);
+  void finish(Request& r);
+};
+
+}  // namespace tnbp
