@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Estimator solves/s on one B200 (or N replicas), mixed vs plain FP64 path.
+
+Workload (default, the 16x16 kicked-Ising solve): open 16x16 square-lattice
+PEPS in |0...0>, 20 Floquet steps of RZZ(theta_J = -pi/4) on every edge then
+RX(theta_h) on every site (theta_h ~ U[0.2, 1.2] from the seed), chi = 16
+(BP at bond dimension 32), BP tolerance 1e-8 / 50 sweeps, sv_min 1e-8;
+observable (1/256) sum_i Z_i + 32 random distinct nearest-neighbour Z Z terms
+(coefficient 1).  Synthetic input: the reference's public inputs are
+generated, not loaded.
+
+One step = one full solve (absorb + BP + truncation for every Floquet step,
+then the FP64 sum of the Pauli terms).  `value` = solves/s of the mixed
+(complex64) path with the problem resident on the device; `e2e` = the same
+through the public API from host data (lattice, TPO and terms uploaded,
+result read back each solve).  The plain complex128 path is timed on one
+solve beside it and |dE| between the two is reported.  Site tensors at
+BP time (~3 GB c64, 6 GB c128) exceed the 126 MB L2, so no flush is needed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank solves its own replica:
+the path does not shard (replicas only); value = N*K solves / max-rank time.
+--impl reference times the reference's own algorithm on the host cores
+(oracle/_ref/estimator: the unchanged tnbp estimator app on the project's
+CPU tensor backend) on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L_SIDE, CHI, STEPS = 16, 16, 20
+THETA_J = -math.pi / 4
+BP_TOL, BP_MAXIT, SV_MIN = 1e-8, 50, 1e-8
+SEED = 20261203
+CPU_SAMPLE_STEPS = 5  # Floquet steps of the CPU reference sample
+
+
+def workload(seed=SEED):
+    rng = np.random.default_rng(seed)
+    theta_h = float(rng.uniform(0.2, 1.2))
+    n = L_SIDE * L_SIDE
+    edges = []
+    for iy in range(L_SIDE):
+        for ix in range(L_SIDE):
+            s = ix + L_SIDE * iy
+            if ix + 1 < L_SIDE:
+                edges.append((s, s + 1))
+            if iy + 1 < L_SIDE:
+                edges.append((s, s + L_SIDE))
+    zz = rng.choice(len(edges), size=32, replace=False)
+    lines = [f"{1.0 / n!r} " + "".join("Z" if n - 1 - k == i else "I" for k in range(n)) for i in range(n)]
+    for m in sorted(int(x) for x in zz):
+        a, b = edges[m]
+        lines.append("1.0 " + "".join("Z" if n - 1 - k in (a, b) else "I" for k in range(n)))
+    return theta_h, "\n".join(lines) + "\n"
+
+
+def kicked_ising_qasm(steps, theta_j, theta_h):
+    n = L_SIDE * L_SIDE
+    out = ["OPENQASM 2.0;", 'include "qelib1.inc";', f"qreg q[{n}];"]
+    for _ in range(steps):
+        for iy in range(L_SIDE):
+            for ix in range(L_SIDE - 1):
+                i = ix + L_SIDE * iy
+                out.append(f"rzz({theta_j!r}) q[{i}],q[{i + 1}];")
+        for iy in range(L_SIDE - 1):
+            for ix in range(L_SIDE):
+                i = ix + L_SIDE * iy
+                out.append(f"rzz({theta_j!r}) q[{i}],q[{i + L_SIDE}];")
+        for i in range(n):
+            out.append(f"rx({theta_h!r}) q[{i}];")
+        out.append("barrier q;")
+    return "\n".join(out) + "\n"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.rows, self.p = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.p = None
+        return self
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def solve(tb, precision, theta_h, pauli_text, resident=None, events=None):
+    """One estimator solve.  Returns (sum, per-solve stats).  With `resident`
+    the state and TPO were created beforehand (device-resident inputs)."""
+    import torch
+    h2d = d2h = 0
+    if resident is None:
+        edges = tb.bond_square_lattice(L_SIDE, L_SIDE)
+        layer = tb.KickedIsingTPO(edges, THETA_J / 2, 0.0, theta_h / 2, 1.0)
+        st = tb.State(edges, precision)
+        tpo = st.tpo(layer)
+        terms = tb.load_sparse_pauli(pauli_text, edges)
+        h2d += len(edges) * 8 + layer.op_data.nbytes + layer.edge_rank.nbytes + layer.op_offset.nbytes
+        h2d += len(terms) * (4 * 3 + 2 + 16)
+    else:
+        st, tpo, terms = resident
+    if events is not None:
+        torch.cuda.synchronize()
+        events.append(torch.cuda.Event(enable_timing=True))
+        events[-1].record()
+    sweeps = 0
+    for _ in range(STEPS):
+        tb.AbsorbTPO(st, tpo)
+        it, _ = tb.BeliefPropagationLoop(st, BP_TOL, BP_MAXIT)
+        sweeps += it
+        d2h += 8 * (it + 1)
+        tb.Truncation(st, CHI, SV_MIN)
+        d2h += st.ne * 12
+    total, per = tb.MeasurePauliSum(st, terms)
+    d2h += 16 + 16 * len(per)
+    stats = dict(sweeps=sweeps, totals=st.sweep_totals(), h2d=h2d, d2h=d2h)
+    st.close()
+    return total, stats
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import tnbp_b200 as tb
+
+    if not torch.cuda.is_available() or not tb.device_available():
+        raise SystemExit("bench needs a CUDA device")
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local_rank))
+    theta_h, pauli_text = workload()
+    edges = tb.bond_square_lattice(L_SIDE, L_SIDE)
+
+    def make_resident(prec):
+        layer = tb.KickedIsingTPO(edges, THETA_J / 2, 0.0, theta_h / 2, 1.0)
+        st = tb.State(edges, prec)
+        return st, st.tpo(layer), tb.load_sparse_pauli(pauli_text, edges)
+
+    # warm-up (untimed): same work as a timed step
+    for _ in range(args.warmup):
+        solve(tb, tb.C64, theta_h, pauli_text)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = tb.kernel_launches()
+    ev_e2e0, ev_res, ev_end = [], [], []
+    sums, stats = [], []
+    with ClockSampler(local_rank) as clk:
+        t_wall = time.perf_counter()
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ev_e2e0.append(e0)
+            s, stt = solve(tb, tb.C64, theta_h, pauli_text, events=ev_res)
+            torch.cuda.synchronize()
+            e1 = torch.cuda.Event(enable_timing=True)
+            e1.record()
+            ev_end.append(e1)
+            sums.append(s)
+            stats.append(stt)
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches = tb.kernel_launches() - launches0
+    e2e_ms = sum(a.elapsed_time(b) for a, b in zip(ev_e2e0, ev_end))
+    res_ms = sum(a.elapsed_time(b) for a, b in zip(ev_res, ev_end))
+    if dist:
+        t = torch.tensor([e2e_ms, res_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms, res_ms = float(t[0]), float(t[1])
+    if rank != 0:
+        dist.destroy_process_group()
+        return
+    K = args.steps
+    value = world * K / (res_ms / 1e3)
+    e2e_value = world * K / (e2e_ms / 1e3)
+    tot_ms = sum(s["totals"][0] for s in stats)
+    tot_fl = sum(s["totals"][1] for s in stats)
+    tot_by = sum(s["totals"][2] for s in stats)
+    n_sw = sum(s["totals"][3] for s in stats)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    tf_peak = peaks.get("bf16_tflops_sustained") or 1400.0
+    achieved = (tot_fl / n_sw) / ((tot_ms / n_sw) / 1e3) / 1e12 if n_sw else None
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "bp_sweep_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("dram_bytes_per_sweep_c64_16x16_chi16")
+        except (OSError, ValueError):
+            traffic = None
+    line = {
+        "metric": "estimator solves/s (mixed complex64 path; plain FP64 GPU path and |dE| beside)",
+        "value": value,
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": args.warmup,
+        "ms_per_step": res_ms / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "c64 (FP32 products, FP64 sums and FP64 truncation eigensolves)",
+        "data": "synthetic (seeded kicked-Ising circuit and Pauli observable)",
+        "config": {"workload": f"kicked-Ising {L_SIDE}x{L_SIDE} open PEPS, {STEPS} steps, chi={CHI}, "
+                               "RZZ(-pi/4), RX(theta_h)",
+                   "theta_h": theta_h, "seed": SEED, "bp_tol": BP_TOL, "bp_max_iter": BP_MAXIT,
+                   "sv_min": SV_MIN, "observable": "(1/256) sum Z_i + 32 NN ZZ",
+                   "parallelism": f"replicas x{world}",
+                   "l2": "no flush: site tensors at BP time (~3 GB) exceed the 126 MB L2"},
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": stats[-1]["h2d"],
+                "d2h_bytes_per_step": stats[-1]["d2h"]},
+        "gpu_launches": int(launches),
+        "observable": {"mixed": [sums[-1].real, sums[-1].imag]},
+        "bp_sweeps_per_solve": stats[-1]["sweeps"],
+        "wall_s": t_wall,
+        "clocks": clk.summary(),
+    }
+    line["roofline"] = {
+        "kernel": "BP sweep (k_leg_apply + k_gram + k_msg_finalize + k_segmented_sum, one CUDA graph)",
+        "bound": "tensor",
+        "achieved": achieved,
+        "peak": tf_peak,
+        "unit": "TFLOP/s",
+        "frac": (achieved / tf_peak) if achieved else None,
+        "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)" if peaks else "fallback 1.4 PF/s",
+        "traffic": traffic,
+        "algorithmic": {"flops_per_sweep": tot_fl / n_sw if n_sw else None,
+                        "bytes_per_sweep": tot_by / n_sw if n_sw else None,
+                        "sweep_ms": tot_ms / n_sw if n_sw else None,
+                        "hbm_achieved_gbs": (tot_by / n_sw) / ((tot_ms / n_sw) / 1e3) / 1e9 if n_sw else None,
+                        "hbm_peak_gbs": peaks.get("hbm_gbs")},
+    }
+    if not args.no_fp64:
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s64, st64 = solve(tb, tb.C128, theta_h, pauli_text)
+        torch.cuda.synchronize()
+        e1.record()
+        torch.cuda.synchronize()
+        ms64 = e0.elapsed_time(e1)
+        line["plain_fp64"] = {"solves_per_s": 1e3 / ms64, "observable": [s64.real, s64.imag],
+                              "bp_sweeps": st64["sweeps"], "sweep_ms": st64["totals"][0] / max(1, st64["totals"][3])}
+        line["dE_vs_fp64"] = abs(sums[-1] - s64)
+        line["speedup_vs_fp64"] = line["plain_fp64"]["solves_per_s"] and e2e_value / line["plain_fp64"]["solves_per_s"]
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_sample(theta_h)
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def cpu_sample(theta_h, steps=CPU_SAMPLE_STEPS):
+    """The reference's estimator app (oracle/_ref/estimator: unchanged tnbp
+    headers and app on the project's CPU tensor backend, OpenMP threads = all
+    host cores) on the first `steps` Floquet steps of the same workload.
+    value = (steps / 20) / seconds: each sampled Floquet step counted as 1/20
+    of a solve.  The sampled steps run BP at bond dimension <= 16; the later
+    steps at 32 cost far more, so this over-states the CPU's solves/s."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "estimator")
+    if not os.path.exists(exe):
+        return {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": "oracle/_ref/estimator not built"}
+    _, pauli_text = workload()
+    d = tempfile.mkdtemp()
+    qp, pp = os.path.join(d, "c.qasm"), os.path.join(d, "p.txt")
+    open(qp, "w").write(kicked_ising_qasm(steps, THETA_J, theta_h))
+    open(pp, "w").write(pauli_text)
+    env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count()))
+    t = time.perf_counter()
+    subprocess.run([exe, "--circuit", qp, "--sparse_pauli", pp, "--max_bond_dim", str(CHI), "--bp_tolerance",
+                    repr(BP_TOL), "--max_bp_iterations", str(BP_MAXIT), "--sv_min", repr(SV_MIN)],
+                   check=True, capture_output=True, env=env, timeout=1800)
+    dt = time.perf_counter() - t
+    return {"value": (steps / STEPS) / dt, "unit": "solves/s", "cores": os.cpu_count(), "kind": "reference",
+            "seconds": dt,
+            "sample": f"first {steps} of {STEPS} Floquet steps of the same solve (BP at D<=16), "
+                      f"counted as {steps}/{STEPS} of a solve; later steps (D=32) cost ~30x more, "
+                      "so this over-states CPU solves/s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    theta_h, _ = workload()
+    vals = []
+    for _ in range(args.warmup):
+        cpu_sample(theta_h)
+    for _ in range(args.steps):
+        vals.append(cpu_sample(theta_h))
+    v = [x["value"] for x in vals if x["value"]]
+    value = float(np.mean(v)) if v else None
+    line = {
+        "impl": "reference",
+        "metric": "estimator solves/s (mixed complex64 path; plain FP64 GPU path and |dE| beside)",
+        "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": (1e3 / value) if value else None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded kicked-Ising circuit and Pauli observable)",
+        "config": {"workload": "kicked-Ising 16x16 open PEPS, 20 steps, chi=16, RZZ(-pi/4), RX(theta_h)",
+                   "theta_h": theta_h, "seed": SEED},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": os.cpu_count(), "kind": "reference",
+                         "sample": vals[-1]["sample"] if vals else None},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--lattice", type=int, default=L_SIDE,
+                    help="lattice side (default 16; smaller sides are for profiling captures only)")
+    ap.add_argument("--nsteps", type=int, default=STEPS,
+                    help="Floquet steps per solve (default 20; fewer only for profiling captures)")
+    args = ap.parse_args()
+    global L_SIDE, STEPS
+    L_SIDE, STEPS = args.lattice, args.nsteps
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

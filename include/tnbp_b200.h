@@ -175,7 +175,9 @@ int tnbp_bp_condition(tnbp_job* job, double* result);
    stop after the first whose condition is < tol.  Runs each sweep once
    (the condition of sweep k is the distance between sweep k+1 and sweep
    k, so the recomputation is shared).  iters_out = sweeps applied;
-   cond_out = last condition (NaN if max_iter == 0). */
+   cond_out = last condition (NaN if max_iter == 0).  On a TNBP_C64 job the
+   tolerance used is max(tol, 1e-6): the complex64 condition has a rounding
+   floor near 1e-7, and sweeping below it only feeds unstable BP modes. */
 int tnbp_bp_run(tnbp_job* job, double tol, int32_t max_iter, int32_t* iters_out,
                 double* cond_out);
 
@@ -212,6 +214,15 @@ int tnbp_measure_pauli_sum(tnbp_job* job, int64_t n_terms, const int32_t* kind,
    algorithmic flops/bytes of one sweep at the current shapes. */
 int tnbp_sweep_stats(const tnbp_job* job, double* last_sweep_ms, double* flops,
                      double* bytes);
+
+/* Sweep time summed over every sweep whose condition was read back (the BP
+   loop reads each), with the matching algorithmic flops and bytes. */
+int tnbp_sweep_totals(const tnbp_job* job, double* total_ms, double* total_flops,
+                      double* total_bytes, int64_t* n_sweeps);
+
+/* Kernels this process has launched through the library so far (a graph
+   launch counts its kernel nodes). */
+unsigned long long tnbp_kernel_launches(void);
 
 /* ============================ served path =============================== */
 

@@ -77,6 +77,7 @@ _SIGS = {
     "tnbp_measure_2site": [_vp, C.c_int64, _i32p, _f64p, _f64p],
     "tnbp_measure_pauli_sum": [_vp, C.c_int64, _i32p, _i32p, _i32p, C.c_char_p, _f64p, _f64p, _f64p],
     "tnbp_sweep_stats": [_vp, _f64p, _f64p, _f64p],
+    "tnbp_sweep_totals": [_vp, _f64p, _f64p, _f64p, _i64p],
     "tnbp_server_create": [C.c_int32, C.c_uint64, C.c_int32, C.POINTER(_vp)],
     "tnbp_server_destroy": [_vp],
     "tnbp_server_submit_kicked_ising": [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
@@ -89,6 +90,13 @@ for _n, _a in _SIGS.items():
     _f = getattr(lib, _n)
     _f.argtypes = _a
     _f.restype = C.c_int
+lib.tnbp_kernel_launches.argtypes = []
+lib.tnbp_kernel_launches.restype = C.c_ulonglong
+
+
+def kernel_launches():
+    """Kernels launched by this process through the library so far."""
+    return int(lib.tnbp_kernel_launches())
 
 
 def _chk(rc):
@@ -390,6 +398,14 @@ class State:
         _chk(lib.tnbp_sweep_stats(self.h, C.byref(ms), C.byref(fl), C.byref(by)))
         return ms.value, fl.value, by.value
 
+    def sweep_totals(self):
+        """(total ms, total algorithmic flops, total algorithmic bytes, sweeps)
+        over every sweep whose condition was read (CUDA events on the job's
+        stream)."""
+        ms, fl, by, n = C.c_double(), C.c_double(), C.c_double(), C.c_int64()
+        _chk(lib.tnbp_sweep_totals(self.h, C.byref(ms), C.byref(fl), C.byref(by), C.byref(n)))
+        return ms.value, fl.value, by.value, n.value
+
 
 def InitTensorProductState(edges, precision=C128, pdims=None, hbm_budget=0):
     """InitTensorProductState (init.h:18-95): returns the device State."""
@@ -449,6 +465,51 @@ def Measure(state, where, ops):
         _chk(lib.tnbp_measure_2site(state.h, len(where), _p(pr, _i32p), _p(o.view(np.float64), _f64p),
                                     _p(out.view(np.float64), _f64p)))
     return out
+
+
+class Server:
+    """Continuous-batching request loop (tnbp_server_*)."""
+
+    def __init__(self, precision=C64, hbm_budget=0, max_active=64):
+        h = _vp()
+        _chk(lib.tnbp_server_create(precision, int(hbm_budget), max_active, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.tnbp_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit_kicked_ising(self, L, chi, steps, theta_j, theta_h, terms, bp_tol=1e-8, bp_max_iter=50,
+                            sv_min=1e-8):
+        rid = C.c_int64()
+        n = len(terms)
+        co = np.ascontiguousarray(terms.coeff, np.complex128) if n else np.zeros(1, np.complex128)
+        kind = np.ascontiguousarray(terms.kind, np.int32) if n else np.zeros(1, np.int32)
+        q0 = np.ascontiguousarray(terms.q0, np.int32) if n else np.zeros(1, np.int32)
+        q1 = np.ascontiguousarray(terms.q1, np.int32) if n else np.zeros(1, np.int32)
+        _chk(lib.tnbp_server_submit_kicked_ising(self.h, L, chi, steps, theta_j, theta_h, bp_tol, bp_max_iter, sv_min,
+                                                 n, _p(kind, _i32p), _p(q0, _i32p), _p(q1, _i32p),
+                                                 terms.letters if n else b"II", _p(co.view(np.float64), _f64p),
+                                                 C.byref(rid)))
+        return rid.value
+
+    def step(self):
+        a, q, d = C.c_int32(), C.c_int32(), C.c_int32()
+        _chk(lib.tnbp_server_step(self.h, C.byref(a), C.byref(q), C.byref(d)))
+        return a.value, q.value, d.value
+
+    def result(self, rid):
+        out = np.zeros(2, np.float64)
+        pend = C.c_int32()
+        _chk(lib.tnbp_server_result(self.h, rid, _p(out, _f64p), C.byref(pend)))
+        return None if pend.value else complex(out[0], out[1])
 
 
 def MeasurePauliSum(state, terms):

@@ -453,6 +453,19 @@ int tnbp_measure_pauli_sum(tnbp_job* job, int64_t n, const int32_t* kind, const 
   });
 }
 
+unsigned long long tnbp_kernel_launches(void) { return tnbp::g_launches.load(); }
+
+int tnbp_sweep_totals(const tnbp_job* job, double* total_ms, double* total_flops, double* total_bytes,
+                      int64_t* n_sweeps) {
+  return guard([&] {
+    need(job, "job is NULL");
+    if (total_ms) *total_ms = job->j->total_sweep_ms;
+    if (total_flops) *total_flops = job->j->total_sweep_flops;
+    if (total_bytes) *total_bytes = job->j->total_sweep_bytes;
+    if (n_sweeps) *n_sweeps = job->j->timed_sweeps;
+  });
+}
+
 int tnbp_sweep_stats(const tnbp_job* job, double* ms, double* flops, double* bytes) {
   return guard([&] {
     need(job, "job is NULL");

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -26,6 +27,8 @@
 namespace tnbp {
 
 thread_local std::string g_last_error;
+std::atomic<unsigned long long> g_launches{0};
+void note_launch(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 
 void check_cuda(cudaError_t e, const char* what, const char* file, int line) {
   if (e != cudaSuccess) {
@@ -64,6 +67,22 @@ static void upload_vec(DevBuf& b, const std::vector<T>& v, cudaStream_t s) {
 }
 
 static inline size_t align_elems(size_t n) { return (n + 31) & ~size_t(31); }
+
+// Site tensors are re-laid out at every AbsorbTPO and truncation; keep the
+// stream-ordered pool's memory mapped across synchronizations instead of
+// returning it to the driver each time (the default threshold of 0 makes
+// every large re-allocation map fresh pages).
+void keep_pool_memory() {
+  static bool done = false;
+  if (done) return;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  cudaMemPool_t pool;
+  CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+  uint64_t thr = UINT64_MAX;
+  CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  done = true;
+}
 
 // ------------------------------------------------------------------ graph
 Graph::Graph(const int32_t* e, int64_t n) {
@@ -118,6 +137,7 @@ Job::Job(const int32_t* e, int64_t n, const int32_t* pdims, int precision, cudaS
     throw Error(TNBP_ENOGPU, "no CUDA device visible: the B200 engine has no CPU path");
   }
   esz = prec == TNBP_C128 ? 16 : 8;
+  keep_pool_memory();
   if (s) {
     stream = s;
   } else {
@@ -245,6 +265,7 @@ SweepBatch& SweepBatch::operator=(SweepBatch&& o) noexcept {
     sum_tasks = std::move(o.sum_tasks);
     cond = std::move(o.cond);
     gram_ntask = o.gram_ntask; nmsg = o.nmsg; nsum = o.nsum; gram_nblocks = o.gram_nblocks;
+    nkernels = o.nkernels;
     graph = o.graph;
     o.graph = nullptr;
   }
@@ -511,7 +532,8 @@ static void leg_apply_attr() {
 }
 
 template <typename R>
-static void launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
+static int launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
+  int n = 0;
   for (auto& lv : b.levels) {
     if (lv.ntask == 0) continue;
     if (lv.max_din > 128) throw Error(TNBP_EUNSUPPORTED, "bond dimension above 128 during BP");
@@ -519,6 +541,7 @@ static void launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
     k_leg_apply<R><<<(unsigned)lv.nblocks, kThreads, smem, stream>>>(
         static_cast<const LegTask*>(lv.tasks.p), static_cast<const long long*>(lv.begins.p), lv.ntask, lv.max_din);
     CK(cudaGetLastError());
+    ++n;
   }
   if (b.gram_ntask) {
     k_gram<R><<<(unsigned)b.gram_nblocks, kThreads, 0, stream>>>(
@@ -526,16 +549,18 @@ static void launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
     CK(cudaGetLastError());
     k_msg_finalize<R><<<b.nmsg, kThreads, 0, stream>>>(static_cast<const MsgTask*>(b.msg_tasks.p));
     CK(cudaGetLastError());
+    n += 2;
   }
   if (b.nsum) {
     k_segmented_sum<<<b.nsum, kThreads, 0, stream>>>(static_cast<const SumTask*>(b.sum_tasks.p));
     CK(cudaGetLastError());
+    ++n;
   }
+  return n;
 }
 
-void launch_batch(const SweepBatch& b, int prec, cudaStream_t stream) {
-  if (prec == TNBP_C128) launch_batch_t<double>(b, stream);
-  else launch_batch_t<float>(b, stream);
+int launch_batch(const SweepBatch& b, int prec, cudaStream_t stream) {
+  return prec == TNBP_C128 ? launch_batch_t<double>(b, stream) : launch_batch_t<float>(b, stream);
 }
 
 void prepare_kernels(int prec) {
@@ -551,7 +576,7 @@ void Job::run_sweep(int par) {
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     try {
-      launch_batch(b, prec, stream);
+      b.nkernels = launch_batch(b, prec, stream);
     } catch (...) {
       cudaStreamEndCapture(stream, &graph);
       throw;
@@ -562,6 +587,7 @@ void Job::run_sweep(int par) {
   }
   CK(cudaEventRecord(ev0, stream));
   CK(cudaGraphLaunch(b.graph, stream));
+  note_launch(b.nkernels);
   CK(cudaEventRecord(ev1, stream));
   last_par = par;
   sweeps_run++;
@@ -571,7 +597,13 @@ double Job::read_cond() {
   CK(cudaMemcpyAsync(host_scalar, plan.single[last_par].cond.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
   float ms = 0.f;
-  if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) last_sweep_ms = ms;
+  if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) {
+    last_sweep_ms = ms;
+    total_sweep_ms += ms;
+    total_sweep_flops += plan.flops;
+    total_sweep_bytes += plan.bytes_alg;
+    ++timed_sweeps;
+  }
   return host_scalar[0];
 }
 void Job::bp_sweep() {
@@ -585,7 +617,17 @@ double Job::bp_condition() {
   return read_cond();
 }
 
-void Job::bp_run(double tol, int max_iter, int* iters, double* cond) {
+// The condition of the complex64 path cannot go below its rounding floor
+// (about 1e-7 per sweep for normalized messages); a tolerance under the
+// floor would run every sweep to max_iter and let unstable BP modes grow
+// from rounding noise.  The mixed path therefore stops at
+// max(tol, kC64TolFloor).
+double effective_tol(int prec, double tol) {
+  return prec == TNBP_C64 ? std::max(tol, kC64TolFloor) : tol;
+}
+
+void Job::bp_run(double tol_in, int max_iter, int* iters, double* cond) {
+  const double tol = effective_tol(prec, tol_in);
   *iters = 0;
   *cond = std::nan("");
   if (max_iter <= 0) return;
@@ -660,11 +702,11 @@ void Job::absorb_tpo(const Tpo& tpo) {
   upload_vec(dmt, mt, stream);
   upload_vec(dmb, mb, stream);
   if (prec == TNBP_C128) {
-    k_absorb_sites<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<AbsorbTask*>(dat.p), static_cast<long long*>(dab.p), (int)at.size());
-    k_expand_msgs<double><<<(unsigned)nmb, kThreads, 0, stream>>>(static_cast<MsgExpandTask*>(dmt.p), static_cast<long long*>(dmb.p), (int)mt.size());
+    (k_absorb_sites<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<AbsorbTask*>(dat.p), static_cast<long long*>(dab.p), (int)at.size()), note_launch());
+    (k_expand_msgs<double><<<(unsigned)nmb, kThreads, 0, stream>>>(static_cast<MsgExpandTask*>(dmt.p), static_cast<long long*>(dmb.p), (int)mt.size()), note_launch());
   } else {
-    k_absorb_sites<float><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<AbsorbTask*>(dat.p), static_cast<long long*>(dab.p), (int)at.size());
-    k_expand_msgs<float><<<(unsigned)nmb, kThreads, 0, stream>>>(static_cast<MsgExpandTask*>(dmt.p), static_cast<long long*>(dmb.p), (int)mt.size());
+    (k_absorb_sites<float><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<AbsorbTask*>(dat.p), static_cast<long long*>(dab.p), (int)at.size()), note_launch());
+    (k_expand_msgs<float><<<(unsigned)nmb, kThreads, 0, stream>>>(static_cast<MsgExpandTask*>(dmt.p), static_cast<long long*>(dmb.p), (int)mt.size()), note_launch());
   }
   CK(cudaGetLastError());
   std::swap(V, nV);
@@ -743,10 +785,10 @@ void Job::run_chains(std::vector<ChainEntry>& chains) {
     prepare_kernels(prec);
     if (prec == TNBP_C128) {
       const size_t smem = leg_smem<double>(maxdin);
-      k_leg_apply<double><<<(unsigned)nb, kThreads, smem, stream>>>(static_cast<LegTask*>(dt.p), static_cast<long long*>(db.p), (int)t.size(), maxdin);
+      (k_leg_apply<double><<<(unsigned)nb, kThreads, smem, stream>>>(static_cast<LegTask*>(dt.p), static_cast<long long*>(db.p), (int)t.size(), maxdin), note_launch());
     } else {
       const size_t smem = leg_smem<float>(maxdin);
-      k_leg_apply<float><<<(unsigned)nb, kThreads, smem, stream>>>(static_cast<LegTask*>(dt.p), static_cast<long long*>(db.p), (int)t.size(), maxdin);
+      (k_leg_apply<float><<<(unsigned)nb, kThreads, smem, stream>>>(static_cast<LegTask*>(dt.p), static_cast<long long*>(db.p), (int)t.size(), maxdin), note_launch());
     }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(stream));
@@ -795,8 +837,8 @@ void Job::truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_ou
   }
   DevBuf dtt;
   upload_vec(dtt, tt, stream);
-  if (prec == TNBP_C128) k_truncate_edges<double><<<ne, kThreads, 0, stream>>>(static_cast<TruncTask*>(dtt.p), chi_max, sv_min);
-  else k_truncate_edges<float><<<ne, kThreads, 0, stream>>>(static_cast<TruncTask*>(dtt.p), chi_max, sv_min);
+  if (prec == TNBP_C128) (k_truncate_edges<double><<<ne, kThreads, 0, stream>>>(static_cast<TruncTask*>(dtt.p), chi_max, sv_min), note_launch());
+  else (k_truncate_edges<float><<<ne, kThreads, 0, stream>>>(static_cast<TruncTask*>(dtt.p), chi_max, sv_min), note_launch());
   CK(cudaGetLastError());
   std::vector<int> hkeep(ne), hstatus(ne);
   std::vector<double> herr(ne);
@@ -850,8 +892,8 @@ void Job::truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_ou
   }
   DevBuf ddt;
   upload_vec(ddt, dt, stream);
-  if (prec == TNBP_C128) k_write_diag<double><<<2 * ne, 128, 0, stream>>>(static_cast<DiagTask*>(ddt.p));
-  else k_write_diag<float><<<2 * ne, 128, 0, stream>>>(static_cast<DiagTask*>(ddt.p));
+  if (prec == TNBP_C128) (k_write_diag<double><<<2 * ne, 128, 0, stream>>>(static_cast<DiagTask*>(ddt.p)), note_launch());
+  else (k_write_diag<float><<<2 * ne, 128, 0, stream>>>(static_cast<DiagTask*>(ddt.p)), note_launch());
   CK(cudaGetLastError());
   std::swap(M[0], nM0);
   std::swap(M[1], nM1);
@@ -894,11 +936,11 @@ void Job::normalize_sites() {
   upload_vec(drt, rt, stream);
   upload_vec(drb, rb, stream);
   if (prec == TNBP_C128) {
-    k_sumsq_partial<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<RangeTask*>(drt.p), static_cast<long long*>(drb.p), ns, per_thread);
-    k_scale_ranges<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<RangeTask*>(drt.p), static_cast<long long*>(drb.p), ns, per_thread);
+    (k_sumsq_partial<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<RangeTask*>(drt.p), static_cast<long long*>(drb.p), ns, per_thread), note_launch());
+    (k_scale_ranges<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<RangeTask*>(drt.p), static_cast<long long*>(drb.p), ns, per_thread), note_launch());
   } else {
-    k_sumsq_partial<float><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<RangeTask*>(drt.p), static_cast<long long*>(drb.p), ns, per_thread);
-    k_scale_ranges<float><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<RangeTask*>(drt.p), static_cast<long long*>(drb.p), ns, per_thread);
+    (k_sumsq_partial<float><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<RangeTask*>(drt.p), static_cast<long long*>(drb.p), ns, per_thread), note_launch());
+    (k_scale_ranges<float><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<RangeTask*>(drt.p), static_cast<long long*>(drb.p), ns, per_thread), note_launch());
   }
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(stream));
@@ -1003,10 +1045,10 @@ void Job::compute_envs(const std::vector<int>& sites1, const std::vector<std::pa
   upload_vec(dgb, gb, stream);
   upload_vec(dpt, pt, stream);
   if (!gt.empty()) {
-    if (prec == TNBP_C128) k_gram<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<GramTask*>(dgt.p), static_cast<long long*>(dgb.p), (int)gt.size());
-    else k_gram<float><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<GramTask*>(dgt.p), static_cast<long long*>(dgb.p), (int)gt.size());
+    if (prec == TNBP_C128) (k_gram<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<GramTask*>(dgt.p), static_cast<long long*>(dgb.p), (int)gt.size()), note_launch());
+    else (k_gram<float><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<GramTask*>(dgt.p), static_cast<long long*>(dgb.p), (int)gt.size()), note_launch());
     CK(cudaGetLastError());
-    k_partial_sum<<<(unsigned)pt.size(), kThreads, 0, stream>>>(static_cast<PartialSumTask*>(dpt.p));
+    (k_partial_sum<<<(unsigned)pt.size(), kThreads, 0, stream>>>(static_cast<PartialSumTask*>(dpt.p)), note_launch());
     CK(cudaGetLastError());
   }
   CK(cudaStreamSynchronize(stream));
@@ -1066,8 +1108,8 @@ void Job::measure_terms(const std::vector<TermSpec>& terms, double* values, doub
   dvals.alloc(std::max<size_t>(terms.size(), 1) * sizeof(double2), stream);
   dsum.alloc(sizeof(double2), stream);
   if (!tt.empty()) {
-    k_terms<<<(unsigned)tt.size(), kThreads, 0, stream>>>(static_cast<TermTask*>(dtt.p), static_cast<double2*>(dvals.p));
-    k_weighted_sum<<<1, kThreads, 0, stream>>>(static_cast<TermTask*>(dtt.p), static_cast<double2*>(dvals.p), (int)tt.size(), static_cast<double2*>(dsum.p));
+    (k_terms<<<(unsigned)tt.size(), kThreads, 0, stream>>>(static_cast<TermTask*>(dtt.p), static_cast<double2*>(dvals.p)), note_launch());
+    (k_weighted_sum<<<1, kThreads, 0, stream>>>(static_cast<TermTask*>(dtt.p), static_cast<double2*>(dvals.p), (int)tt.size(), static_cast<double2*>(dsum.p)), note_launch());
     CK(cudaGetLastError());
   }
   std::vector<double> hv(2 * std::max<size_t>(terms.size(), 1), 0.0);

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <stdexcept>
@@ -19,6 +20,7 @@ struct Error : std::runtime_error {
 };
 
 extern thread_local std::string g_last_error;
+extern std::atomic<unsigned long long> g_launches;
 void check_cuda(cudaError_t e, const char* what, const char* file, int line);
 #define CK(x) ::tnbp::check_cuda((x), #x, __FILE__, __LINE__)
 
@@ -72,6 +74,7 @@ struct SweepBatch {
   DevBuf gram_tasks, gram_begins, msg_tasks, sum_tasks, cond;
   int gram_ntask = 0, nmsg = 0, nsum = 0;
   long long gram_nblocks = 0;
+  int nkernels = 0;
   cudaGraphExec_t graph = nullptr;
   SweepBatch() = default;
   SweepBatch(const SweepBatch&) = delete;
@@ -102,7 +105,11 @@ struct SweepPlan {
 struct Job;
 struct BatchEntry { Job* job; int parity; };
 void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStream_t stream);
-void launch_batch(const SweepBatch& b, int prec, cudaStream_t stream);
+int launch_batch(const SweepBatch& b, int prec, cudaStream_t stream);
+void note_launch(int n = 1);
+void keep_pool_memory();
+constexpr double kC64TolFloor = 1e-6;
+double effective_tol(int prec, double tol);
 void prepare_kernels(int prec);
 
 // A TPO layer on the device: complex128 op tensors of shape
@@ -144,6 +151,8 @@ struct Job {
   SweepPlan plan;
   long long sweeps_run = 0;
   float last_sweep_ms = 0.f;
+  double total_sweep_ms = 0.0, total_sweep_flops = 0.0, total_sweep_bytes = 0.0;
+  long long timed_sweeps = 0;
 
   Job(const int32_t* e, int64_t n, const int32_t* pdims, int precision, cudaStream_t s, uint64_t budget);
   ~Job();

@@ -603,6 +603,9 @@ static void small_svd(int m, int n, const std::vector<cd>& A, std::vector<cd>& U
     }
   std::vector<cd> V(N * N, 0.0);
   for (int i = 0; i < N; ++i) V[i + N * i] = 1.0;
+  double fro = 0;
+  for (auto& x : W) fro += std::norm(x);
+  const double eps = 2.220446049250313e-16, tol = eps * std::max(M, 8);
   for (int sweep = 0; sweep < 80; ++sweep) {
     bool rot = false;
     for (int i = 0; i < N - 1; ++i)
@@ -615,11 +618,13 @@ static void small_svd(int m, int n, const std::vector<cd>& A, std::vector<cd>& U
           ga += std::conj(W[r + M * i]) * W[r + M * j];
         }
         const double g = std::abs(ga);
-        if (!(g > 0) || g <= 1e-15 * std::sqrt(al * be)) continue;
-        rot = true;
+        // numerically-zero columns (rank-deficient gates) are not rotated
+        if (!(g > 0) || g <= tol * std::sqrt(al * be) || std::min(al, be) <= tol * tol * fro) continue;
         const cd ph = ga / g;
         const double z = (be - al) / (2 * g);
         const double t = (z >= 0 ? 1.0 : -1.0) / (std::abs(z) + std::sqrt(1 + z * z));
+        if (std::abs(t) < eps) continue;
+        rot = true;
         const double c = 1 / std::sqrt(1 + t * t), sn = c * t;
         for (int r = 0; r < M; ++r) {
           const cd x = W[r + M * i], y = W[r + M * j];

@@ -36,6 +36,7 @@ Server::Server(int precision, uint64_t budget_bytes, int max_active_jobs)
     cudaGetLastError();
     throw Error(TNBP_ENOGPU, "no CUDA device visible: the B200 engine has no CPU path");
   }
+  keep_pool_memory();
   CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   if (budget == 0) {
     size_t fr = 0, tot = 0;
@@ -179,7 +180,7 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
     for (auto* r : inbp) if (!r->job->plan.valid) r->job->build_plan();
     prepare_kernels(prec);
     build_batch(entries, batch, stream);
-    launch_batch(batch, prec, stream);
+    note_launch(launch_batch(batch, prec, stream));
     if (hcond_cap < entries.size()) {
       if (hcond) cudaFreeHost(hcond);
       hcond_cap = std::max<size_t>(64, 2 * entries.size());
@@ -196,7 +197,7 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
         continue;
       }
       const double c = hcond[i];
-      if (c < r.tol || r.bp_iters >= r.maxit) {
+      if (c < effective_tol(prec, r.tol) || r.bp_iters >= r.maxit) {
         r.phase = Request::TRUNC;  // keep the current messages
       } else {
         j.cur = 1 - j.cur;

@@ -48,12 +48,23 @@ __device__ __forceinline__ double warp_sum1(double v) {
 // One-sided Jacobi on the n x n matrix A (column-major); V accumulates the
 // rotations so that A_in = A_out * V^H.  Returns sweeps used, -1 if the
 // sweep limit was reached.
-__device__ int block_jacobi(double2* A, double2* V, int n, int* flag) {
-  for (int i = threadIdx.x; i < n * n; i += blockDim.x)
+__device__ int block_jacobi(double2* A, double2* V, int n, int* flag, double* red) {
+  double fro = 0.0;
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
     V[i] = (i % n == i / n) ? make_double2(1.0, 0.0) : make_double2(0.0, 0.0);
+    fro += abs2(A[i]);
+  }
+  fro = block_sum(fro, red);
   const int np = n + (n & 1);
   const int nwarps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const double tol = 1e-15;
+  // Pairs count as orthogonal once |a_i^H a_j| <= n eps |a_i| |a_j|: the
+  // rounding of the dot product itself is about sqrt(n) eps, so a tighter
+  // threshold could keep rotating noise forever.  A column whose norm is at
+  // the rounding level of the matrix (<= n eps ||A||_F) is numerically zero
+  // and is not rotated (its singular value is noise, far below any cut).
+  const double eps = 2.220446049250313e-16;
+  const double tol = eps * (double)max(n, 8);
+  const double zero2 = (tol * tol) * fro;
   for (int sweep = 0; sweep < kSvdMaxSweeps; ++sweep) {
     __syncthreads();
     if (threadIdx.x == 0) *flag = 0;
@@ -79,11 +90,12 @@ __device__ int block_jacobi(double2* A, double2* V, int n, int* flag) {
         be = warp_sum1(be);
         ga = warp_sum2(ga);
         const double g = sqrt(abs2(ga));
-        if (!(g > 0.0) || g <= tol * sqrt(al * be)) continue;
-        if (lane == 0) *flag = 1;
+        if (!(g > 0.0) || g <= tol * sqrt(al * be) || min(al, be) <= zero2) continue;
         const double2 ph = make_double2(ga.x / g, ga.y / g);
         const double zeta = (be - al) / (2.0 * g);
         const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        if (fabs(t) < eps) continue;  // the rotation would not change a bit
+        if (lane == 0) *flag = 1;
         const double c = 1.0 / sqrt(1.0 + t * t);
         const double s = c * t;
         const double2 sph = s * ph, sphc = s * conj(ph);
@@ -134,8 +146,8 @@ __device__ void block_sv_sort(const double2* A, int n, double* s_tmp, double* s,
 // R and S written (D x D).  U/V factors taken from the Jacobi result.
 __device__ void block_sqrt_inv(double2* A, double2* V, int n, double sv_min, double* s_tmp,
                                double* s, int* perm, double2* Rout, double2* Sout, int* flag,
-                               int* status) {
-  if (block_jacobi(A, V, n, flag) < 0 && threadIdx.x == 0) *status = 1;
+                               int* status, double* red) {
+  if (block_jacobi(A, V, n, flag, red) < 0 && threadIdx.x == 0) *status = 1;
   block_sv_sort(A, n, s_tmp, s, perm);
   const double sq_min = sqrt(sv_min);
   // R[i,j] = sum_k U[i,k] sq_k conj(V[j,k]);  U[:,k] = A[:,perm k] / s_k
@@ -181,10 +193,10 @@ __global__ void __launch_bounds__(kThreads) k_truncate_edges(const TruncTask* __
   const C* Ma = static_cast<const C*>(tk.Ma);
   const C* Mb = static_cast<const C*>(tk.Mb);
   for (long long i = threadIdx.x; i < nn; i += kThreads) W0[i] = to_d2(Ma[i]);
-  block_sqrt_inv(W0, W1, n, sv_min, s_tmp, tk.sv, tk.perm, RA, SA, &flag, tk.status);
+  block_sqrt_inv(W0, W1, n, sv_min, s_tmp, tk.sv, tk.perm, RA, SA, &flag, tk.status, red);
   for (long long i = threadIdx.x; i < nn; i += kThreads) W0[i] = to_d2(Mb[i]);
   __syncthreads();
-  block_sqrt_inv(W0, W1, n, sv_min, s_tmp, tk.sv + n, tk.perm + n, RB, SB, &flag, tk.status);
+  block_sqrt_inv(W0, W1, n, sv_min, s_tmp, tk.sv + n, tk.perm + n, RB, SB, &flag, tk.status, red);
   // T = RA^T RB, normalized (truncation.h:110-121)
   double ss = 0.0;
   for (long long idx = threadIdx.x; idx < nn; idx += kThreads) {
@@ -200,7 +212,7 @@ __global__ void __launch_bounds__(kThreads) k_truncate_edges(const TruncTask* __
   __syncthreads();
   double* sT = tk.sv + 2 * n;
   int* pT = tk.perm + 2 * n;
-  if (block_jacobi(W0, W1, n, &flag) < 0 && threadIdx.x == 0) *tk.status = 1;
+  if (block_jacobi(W0, W1, n, &flag, red) < 0 && threadIdx.x == 0) *tk.status = 1;
   block_sv_sort(W0, n, s_tmp, sT, pT);
   int keep = 0;
   while (keep < n && keep < chi_max && sT[keep] > sv_min) ++keep;
