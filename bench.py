@@ -59,7 +59,7 @@ def workload(seed=SEED):
                 edges.append((s, s + 1))
             if iy + 1 < L_SIDE:
                 edges.append((s, s + L_SIDE))
-    zz = rng.choice(len(edges), size=32, replace=False)
+    zz = rng.choice(len(edges), size=min(32, len(edges)), replace=False)
     lines = [f"{1.0 / n!r} " + "".join("Z" if n - 1 - k == i else "I" for k in range(n)) for i in range(n)]
     for m in sorted(int(x) for x in zz):
         a, b = edges[m]
@@ -361,6 +361,7 @@ def run_reference(args, rank, world):
 
 
 def main():
+    global L_SIDE, STEPS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
@@ -373,7 +374,6 @@ def main():
     ap.add_argument("--nsteps", type=int, default=STEPS,
                     help="Floquet steps per solve (default 20; fewer only for profiling captures)")
     args = ap.parse_args()
-    global L_SIDE, STEPS
     L_SIDE, STEPS = args.lattice, args.nsteps
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
