@@ -224,6 +224,32 @@ int tnbp_sweep_totals(const tnbp_job* job, double* total_ms, double* total_flops
    launch counts its kernel nodes). */
 unsigned long long tnbp_kernel_launches(void);
 
+/* No counterpart in the reference.  One directed BP message (the arithmetic
+   of bp.h:128-175 for one site and one target leg) with NO device
+   allocation, for callers that may not call cudaMalloc: code running inside
+   a framework that owns the whole device-memory budget (a pre-reserved arena
+   or an allocator that accounts for every byte) and code on a
+   stream-ordered pipeline that cannot take cudaMalloc's implicit device
+   synchronization.  Its scratch is one static device array of about 36 MiB
+   that every GPU loading the library holds until exit; the caller passes
+   device pointers to the inputs and the output:
+     site      complex128 site tensor, column-major, shape[rank] with the
+               physical leg last (at most TNBP_NOALLOC_MAX_SITE_ELEMS
+               elements, bond dims <= 128; larger inputs are rejected with
+               TNBP_EINVAL before any GPU work)
+     msgs_in   host array of rank-1 device pointers: the incoming D_k x D_k
+               message on each leg k (the entry for the target is ignored)
+     msg_out   device pointer to D_t x D_t complex128: the normalized message
+   The first call on a device looks up the scratch array's device address
+   (cudaGetSymbolAddress) with that device current; make that first call
+   before any stream capture.  Every call on a device shares the one array
+   and overwrites it (nothing in it needs to start at zero), so calls whose
+   GPU work overlaps race: order them on one stream or synchronize. */
+#define TNBP_NOALLOC_MAX_SITE_ELEMS 1048576
+int tnbp_bp_message_noalloc(const double* site, const int32_t* shape, int32_t rank,
+                            int32_t target, const double* const* msgs_in, double* msg_out,
+                            void* stream);
+
 /* ============================ served path =============================== */
 
 typedef struct tnbp_server tnbp_server;
