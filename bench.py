@@ -6,7 +6,8 @@ PEPS in |0...0>, 20 Floquet steps of RZZ(theta_J = -pi/4) on every edge then
 RX(theta_h) on every site (theta_h ~ U[0.2, 1.2] from the seed), chi = 16
 (BP at bond dimension 32), BP tolerance 1e-8 / 50 sweeps, sv_min 1e-8;
 observable (1/256) sum_i Z_i + 32 random distinct nearest-neighbour Z Z terms
-(coefficient 1).  Synthetic input: the reference's public inputs are
+(coefficient 1).  The seed (25, theta_h = 0.3607) is one whose draw lies in
+the regime where loopy BP converges on this lattice (see SEED).  Synthetic input: the reference's public inputs are
 generated, not loaded.
 
 One step = one full solve (absorb + BP + truncation for every Floquet step,
@@ -43,7 +44,11 @@ sys.path.insert(0, ROOT)
 L_SIDE, CHI, STEPS = 16, 16, 20
 THETA_J = -math.pi / 4
 BP_TOL, BP_MAXIT, SV_MIN = 1e-8, 50, 1e-8
-SEED = 20261203
+# theta_h ~ U[0.2, 1.2] from this seed: 0.3607.  The first seed tried
+# (20261203, theta_h = 1.038) is outside the regime where loopy BP converges
+# on this lattice: from step 7 on its condition never reaches 1e-8 and grows
+# after its minimum, so every step runs 50 sweeps and the messages are noise.
+SEED = 25
 CPU_SAMPLE_STEPS = 5  # Floquet steps of the CPU reference sample
 
 

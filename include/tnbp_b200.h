@@ -176,8 +176,10 @@ int tnbp_bp_condition(tnbp_job* job, double* result);
    (the condition of sweep k is the distance between sweep k+1 and sweep
    k, so the recomputation is shared).  iters_out = sweeps applied;
    cond_out = last condition (NaN if max_iter == 0).  On a TNBP_C64 job the
-   tolerance used is max(tol, 1e-6): the complex64 condition has a rounding
-   floor near 1e-7, and sweeping below it only feeds unstable BP modes. */
+   tolerance used is max(tol, 1e-6) and the loop also stops at the first
+   sweep whose condition is larger than the previous one: the complex64
+   condition has a rounding floor near 1e-7, and sweeping past the minimum
+   only feeds unstable BP modes. */
 int tnbp_bp_run(tnbp_job* job, double tol, int32_t max_iter, int32_t* iters_out,
                 double* cond_out);
 

@@ -626,6 +626,11 @@ double effective_tol(int prec, double tol) {
   return prec == TNBP_C64 ? std::max(tol, kC64TolFloor) : tol;
 }
 
+// The mixed path also stops as soon as the condition grows: past the
+// minimum the unstable BP mode amplifies rounding noise every sweep (the
+// plain path keeps the reference's rule exactly).
+bool stop_on_growth(int prec) { return prec == TNBP_C64; }
+
 void Job::bp_run(double tol_in, int max_iter, int* iters, double* cond) {
   const double tol = effective_tol(prec, tol_in);
   *iters = 0;
@@ -634,12 +639,15 @@ void Job::bp_run(double tol_in, int max_iter, int* iters, double* cond) {
   run_sweep(cur);
   cur = 1 - cur;
   *iters = 1;
+  double prev = INFINITY;
   while (true) {
     run_sweep(cur);
     const double c = read_cond();
     *cond = c;
     if (c < tol) break;
     if (*iters >= max_iter) break;
+    if (stop_on_growth(prec) && c > prev) break;
+    prev = c;
     cur = 1 - cur;
     ++*iters;
   }

@@ -110,6 +110,7 @@ void note_launch(int n = 1);
 void keep_pool_memory();
 constexpr double kC64TolFloor = 1e-6;
 double effective_tol(int prec, double tol);
+bool stop_on_growth(int prec);
 void prepare_kernels(int prec);
 
 // A TPO layer on the device: complex128 op tensors of shape

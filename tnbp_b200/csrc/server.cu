@@ -163,6 +163,7 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
       r.job->absorb_tpo(*r.tpo);
       r.phase = Request::BP;
       r.bp_iters = 0;
+      r.prev_cond = INFINITY;
       if (r.maxit <= 0) r.phase = Request::TRUNC;
     }
   }
@@ -197,9 +198,10 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
         continue;
       }
       const double c = hcond[i];
-      if (c < effective_tol(prec, r.tol) || r.bp_iters >= r.maxit) {
+      if (c < effective_tol(prec, r.tol) || r.bp_iters >= r.maxit || (stop_on_growth(prec) && c > r.prev_cond)) {
         r.phase = Request::TRUNC;  // keep the current messages
       } else {
+        r.prev_cond = c;
         j.cur = 1 - j.cur;
         ++r.bp_iters;
       }

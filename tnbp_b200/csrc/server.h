@@ -25,6 +25,7 @@ struct Request {
   std::unique_ptr<Job> job;
   std::unique_ptr<Tpo> tpo;
   int step = 0, bp_iters = 0;
+  double prev_cond = 0;
   uint64_t footprint = 0;
   double result[2] = {0, 0};
 };
