@@ -10,6 +10,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -22,6 +23,7 @@
 #include "engine.h"
 #include "kernels.cuh"
 #include "measure.cuh"
+#include "tc_leg.cuh"
 #include "truncate.cuh"
 
 namespace tnbp {
@@ -481,6 +483,28 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
     b.levels[lv].ntask = (int)t.size();
     b.levels[lv].nblocks = nb;
     b.levels[lv].max_din = maxdin;
+    // complex64 levels whose dims fit the tcgen05 kernel run on the tensor cores
+    int maxdout = 1;
+    for (auto& lt : t) maxdout = std::max(maxdout, lt.Dout);
+    if (!entries.empty() && entries[0].job->prec == TNBP_C64 && tcgen05_enabled() && maxdin <= tc::kTcMaxD &&
+        maxdout <= tc::kTcMaxD && !t.empty()) {
+      std::vector<LegTask> t2 = t;
+      std::vector<long long> b2;
+      long long nb2 = 0;
+      int dp = 4, dq = 8;
+      for (auto& lt : t2) {
+        lt.block_begin = nb2;
+        b2.push_back(nb2);
+        nb2 += (lt.L * lt.R + tc::kTcRows - 1) / tc::kTcRows;
+        dp = std::max(dp, (lt.Din + 3) & ~3);
+        dq = std::max(dq, (lt.Dout + 7) & ~7);
+      }
+      upload_vec(b.levels[lv].tc_tasks, t2, stream);
+      upload_vec(b.levels[lv].tc_begins, b2, stream);
+      b.levels[lv].tc_nblocks = nb2;
+      b.levels[lv].tc_smem = tc::leg_smem_bytes();
+      b.levels[lv].use_tc = true;
+    }
   }
   std::vector<GramTask> gt;
   std::vector<long long> gb;
@@ -536,6 +560,16 @@ static int launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
   int n = 0;
   for (auto& lv : b.levels) {
     if (lv.ntask == 0) continue;
+    if (lv.use_tc) {
+      // persistent: up to 2 CTAs per SM, each over a contiguous range of tiles
+      const long long grid = std::min<long long>(lv.tc_nblocks, 2LL * num_sms());
+      k_leg_apply_tc<<<(unsigned)grid, 128, lv.tc_smem, stream>>>(
+          static_cast<const LegTask*>(lv.tc_tasks.p), static_cast<const long long*>(lv.tc_begins.p), lv.ntask,
+          lv.tc_nblocks);
+      CK(cudaGetLastError());
+      ++n;
+      continue;
+    }
     if (lv.max_din > 128) throw Error(TNBP_EUNSUPPORTED, "bond dimension above 128 during BP");
     const size_t smem = leg_smem<R>(lv.max_din);
     k_leg_apply<R><<<(unsigned)lv.nblocks, kThreads, smem, stream>>>(
@@ -564,8 +598,51 @@ int launch_batch(const SweepBatch& b, int prec, cudaStream_t stream) {
 }
 
 void prepare_kernels(int prec) {
-  if (prec == TNBP_C128) leg_apply_attr<double>();
-  else leg_apply_attr<float>();
+  if (prec == TNBP_C128) {
+    leg_apply_attr<double>();
+  } else {
+    leg_apply_attr<float>();
+    static bool tc_done = false;
+    if (!tc_done) {
+      CK(cudaFuncSetAttribute(k_leg_apply_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)tc::leg_smem_bytes()));
+      tc_done = true;
+    }
+  }
+}
+
+int num_sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+  }
+  return n;
+}
+
+// The tcgen05 leg kernel serves complex64 levels with dims <= 32; setting
+// TNBP_DISABLE_TCGEN05=1 routes them to the CUDA-core kernel instead (both do
+// the full contraction; used to compare the two).
+bool tcgen05_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("TNBP_DISABLE_TCGEN05");
+    return !(e && e[0] == '1');
+  }();
+  return on;
+}
+
+// A tcgen05 CTA that gave up waiting for its MMAs records it in g_tc_error.
+void check_tc_error(cudaStream_t stream) {
+  int err = 0;
+  CK(cudaMemcpyFromSymbolAsync(&err, g_tc_error, sizeof(int), 0, cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  if (err) {
+    const int zero = 0;
+    CK(cudaMemcpyToSymbolAsync(g_tc_error, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+    throw Error(TNBP_ECUDA, "a tcgen05 tile reached its wait limit (MMA completion not observed)");
+  }
 }
 
 void Job::run_sweep(int par) {
@@ -596,6 +673,7 @@ void Job::run_sweep(int par) {
 double Job::read_cond() {
   CK(cudaMemcpyAsync(host_scalar, plan.single[last_par].cond.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
+  if (prec == TNBP_C64) check_tc_error(stream);
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) {
     last_sweep_ms = ms;
@@ -610,6 +688,7 @@ void Job::bp_sweep() {
   run_sweep(cur);
   cur = 1 - cur;
   CK(cudaStreamSynchronize(stream));
+  if (prec == TNBP_C64) check_tc_error(stream);
 }
 
 double Job::bp_condition() {

@@ -69,7 +69,17 @@ struct LevelHost {
 // per-job path, captured once per parity as a CUDA graph) or from many jobs
 // at once (the served path: every active job's sweep in the same launches).
 struct SweepBatch {
-  struct Level { DevBuf tasks, begins; int ntask = 0; long long nblocks = 0; int max_din = 1; };
+  struct Level {
+    DevBuf tasks, begins;
+    int ntask = 0;
+    long long nblocks = 0;
+    int max_din = 1;
+    // tcgen05 path (complex64, all dims <= 32): 128-row tiles
+    bool use_tc = false;
+    DevBuf tc_tasks, tc_begins;
+    long long tc_nblocks = 0;
+    size_t tc_smem = 0;
+  };
   std::vector<Level> levels;
   DevBuf gram_tasks, gram_begins, msg_tasks, sum_tasks, cond;
   int gram_ntask = 0, nmsg = 0, nsum = 0;
@@ -112,6 +122,9 @@ constexpr double kC64TolFloor = 1e-6;
 double effective_tol(int prec, double tol);
 bool stop_on_growth(int prec);
 void prepare_kernels(int prec);
+bool tcgen05_enabled();
+int num_sms();
+void check_tc_error(cudaStream_t stream);
 
 // A TPO layer on the device: complex128 op tensors of shape
 // (r_leg0..r_leg{g-1}, d, d') per site.

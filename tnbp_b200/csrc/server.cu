@@ -189,6 +189,7 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
     }
     CK(cudaMemcpyAsync(hcond, batch.cond.p, entries.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
+    if (prec == TNBP_C64) check_tc_error(stream);
     for (size_t i = 0; i < inbp.size(); ++i) {
       Request& r = *inbp[i];
       Job& j = *r.job;

@@ -1,0 +1,278 @@
+// Leg contraction on the 5th-generation tensor cores (tcgen05, sm_100a) for
+// the complex64 path:  out[l, k, r] = sum_j in[l, j, r] * M[j, k].
+//
+// A CTA (128 threads) works through 128-row tiles, rows q = l + L*r.  The complex
+// product is one real GEMM
+//     [A_re | A_im] (128 x 2Dp)  x  [[M_re, M_im], [-M_im, M_re]] (2Dp x 2Dq)
+//   = [C_re | C_im] (128 x 2Dq)
+// in TF32 with the 3xTF32 split x = hi + lo (hi = tf32(x), lo = tf32(x - hi)):
+// C = A_hi B_hi + A_hi B_lo + A_lo B_hi, accumulated in FP32 in tensor
+// memory (TMEM).  Operands are written by the threads into shared memory in
+// the canonical K-major, no-swizzle UMMA layout (8-row x 16-byte core
+// matrices), one thread issues tcgen05.mma, tcgen05.commit arrives on an
+// mbarrier, and each warp reads its 32 accumulator lanes back with
+// tcgen05.ld.  Dp = Din rounded up to 4, Dq = Dout rounded up to 8
+// (zero padded); Din, Dout <= 32.
+//
+// Every wait is bounded: on timeout the CTA records an error in
+// g_tc_error, waits once more (bounded) for MMAs in flight, skips its
+// epilogue, frees its TMEM and returns.
+#pragma once
+#include <cstdint>
+
+#include "kernels.cuh"
+
+namespace tnbp {
+
+__device__ int g_tc_error = 0;
+
+namespace tc {
+
+constexpr int kTcRows = 128;
+constexpr int kTcMaxD = 32;
+constexpr long long kWaitLimit = 1ll << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// UMMA shared-memory descriptor: start address, leading (K-direction core
+// matrix) byte offset, stride (8-row group) byte offset, version 1, no swizzle.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// Instruction descriptor, kind::tf32: D F32, A/B TF32, both K-major.
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ float to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// Byte offset of element (row, k) in a canonical K-major operand of R rows.
+__device__ __forceinline__ uint32_t kmajor_off(int row, int k, int R) {
+  return (uint32_t)((k >> 2) * (R * 16) + (row >> 3) * 128 + (row & 7) * 16 + (k & 3) * 4);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase) {
+  for (long long i = 0; i < kWaitLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared memory bytes of one CTA (operands sized for dims up to 32).
+__host__ __device__ constexpr size_t leg_smem_bytes() {
+  return (size_t)2 * kTcRows * (2 * kTcMaxD) * 4 + (size_t)2 * (2 * kTcMaxD) * (2 * kTcMaxD) * 4 + 1024 + 64;
+}
+
+}  // namespace tc
+
+// Persistent over a contiguous range of 128-row tiles: TMEM is allocated
+// once, the B operand is rebuilt only when the tile range crosses into a new
+// task, and the next tile's global loads are issued before waiting for the
+// current tile's MMAs so that loads, tensor-core work and the epilogue
+// overlap.
+__global__ void __launch_bounds__(128) k_leg_apply_tc(const LegTask* __restrict__ tasks,
+                                                      const long long* __restrict__ begins, int ntask,
+                                                      long long total_tiles) {
+  using namespace tc;
+  extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+  unsigned char* smem = tc_smem_raw + ((1024 - (smem_u32(tc_smem_raw) & 1023)) & 1023);
+  unsigned char* a_hi = smem;                                // 128 x 64 fp32
+  unsigned char* a_lo = a_hi + kTcRows * 2 * kTcMaxD * 4;
+  unsigned char* b_hi = a_lo + kTcRows * 2 * kTcMaxD * 4;    // up to 64 x 64 fp32
+  unsigned char* b_lo = b_hi + (2 * kTcMaxD) * (2 * kTcMaxD) * 4;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(b_lo + (2 * kTcMaxD) * (2 * kTcMaxD) * 4);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  const long long per = (total_tiles + gridDim.x - 1) / gridDim.x;
+  const long long t_begin = (long long)blockIdx.x * per;
+  const long long t_end = min(total_tiles, t_begin + per);
+  if (t_begin >= t_end) return;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(64u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(1u));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  int cur_task = -1;
+  LegTask tk;
+  int Din = 0, Dout = 0, Dp = 4, Dq = 8;
+  float2 nxt[kTcMaxD];
+  // issue the global loads of one tile row (thread = row) into registers
+  auto load_row = [&](long long tile, int task_id) {
+    const LegTask t = tasks[task_id];
+    const long long q = (tile - t.block_begin) * kTcRows + tid;
+    const long long rows = t.L * t.R;
+    const float2* __restrict__ in = static_cast<const float2*>(t.in);
+    if (q < rows) {
+      const long long l = q % t.L, r = q / t.L;
+      const long long base = l + t.L * (long long)t.Din * r;
+#pragma unroll
+      for (int k = 0; k < kTcMaxD; ++k)
+        nxt[k] = k < t.Din ? __ldg(&in[base + t.L * k]) : make_float2(0.f, 0.f);
+    } else {
+#pragma unroll
+      for (int k = 0; k < kTcMaxD; ++k) nxt[k] = make_float2(0.f, 0.f);
+    }
+  };
+  int task_of_next = find_task(begins, ntask, t_begin);
+  load_row(t_begin, task_of_next);
+  uint32_t phase = 0;
+  for (long long tile = t_begin; tile < t_end; ++tile) {
+    const int task_id = task_of_next;
+    if (task_id != cur_task) {
+      cur_task = task_id;
+      tk = tasks[task_id];
+      Din = tk.Din;
+      Dout = tk.Dout;
+      Dp = (Din + 3) & ~3;
+      Dq = (Dout + 7) & ~7;
+      const int K2 = 2 * Dp, N2 = 2 * Dq;
+      const float2* __restrict__ mat = static_cast<const float2*>(tk.mat);
+      // B_real[k2][n2] = [[M_re, M_im], [-M_im, M_re]], stored N2 x K2 K-major
+      for (int n2 = warp; n2 < N2; n2 += 4) {
+        const int nr = n2 < Dq ? n2 : n2 - Dq, pn = n2 < Dq ? 0 : 1;
+        for (int k2 = tid & 31; k2 < K2; k2 += 32) {
+          const int kr = k2 < Dp ? k2 : k2 - Dp, pk = k2 < Dp ? 0 : 1;
+          float v = 0.f;
+          if (kr < Din && nr < Dout) {
+            const float2 m = __ldg(&mat[kr + (long long)Din * nr]);
+            v = (pk == pn) ? m.x : (pk == 0 ? m.y : -m.y);
+          }
+          const float h = to_tf32(v), lo = to_tf32(v - h);
+          *reinterpret_cast<float*>(b_hi + kmajor_off(n2, k2, N2)) = h;
+          *reinterpret_cast<float*>(b_lo + kmajor_off(n2, k2, N2)) = lo;
+        }
+      }
+    }
+    const int K2 = 2 * Dp, N2 = 2 * Dq;
+    // A operand for this tile from the prefetched registers
+#pragma unroll
+    for (int k = 0; k < kTcMaxD; ++k) {
+      if (k < Dp) {
+        const float re = nxt[k].x, im = nxt[k].y;
+        const float rh = to_tf32(re), ih = to_tf32(im);
+        *reinterpret_cast<float*>(a_hi + kmajor_off(tid, k, kTcRows)) = rh;
+        *reinterpret_cast<float*>(a_hi + kmajor_off(tid, Dp + k, kTcRows)) = ih;
+        *reinterpret_cast<float*>(a_lo + kmajor_off(tid, k, kTcRows)) = to_tf32(re - rh);
+        *reinterpret_cast<float*>(a_lo + kmajor_off(tid, Dp + k, kTcRows)) = to_tf32(im - ih);
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+      const uint32_t idesc = idesc_tf32(kTcRows, N2);
+      const uint32_t a_lbo = kTcRows * 16, b_lbo = N2 * 16;
+      const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo), bh = smem_u32(b_hi), bl = smem_u32(b_lo);
+      for (int s = 0; s < K2 / 8; ++s) {
+        const uint32_t ao = (uint32_t)s * 2 * a_lbo, bo = (uint32_t)s * 2 * b_lbo;
+        mma_tf32(tmem, smem_desc(ah + ao, a_lbo, 128), smem_desc(bh + bo, b_lbo, 128), idesc, s > 0 ? 1u : 0u);
+        mma_tf32(tmem, smem_desc(ah + ao, a_lbo, 128), smem_desc(bl + bo, b_lbo, 128), idesc, 1u);
+        mma_tf32(tmem, smem_desc(al + ao, a_lbo, 128), smem_desc(bh + bo, b_lbo, 128), idesc, 1u);
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(mbar))
+                   : "memory");
+    }
+    // prefetch the next tile while the tensor cores work
+    if (tile + 1 < t_end) {
+      task_of_next = (tile + 1 >= tk.block_begin + ((tk.L * tk.R + kTcRows - 1) / kTcRows))
+                         ? find_task(begins, ntask, tile + 1)
+                         : task_id;
+      load_row(tile + 1, task_of_next);
+    }
+    const bool ok = mbar_wait(smem_u32(mbar), phase);
+    // the CTA leaves together if any thread gave up waiting; one more
+    // bounded wait lets MMAs still in flight drain before TMEM is freed
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) atomicExch(&g_tc_error, 1);
+      if (!ok) mbar_wait(smem_u32(mbar), phase);
+      break;
+    }
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // epilogue: warp w holds tile rows 32w..32w+31 in TMEM lanes
+    float c[64];
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    tmem_ld32(lane_addr, c);
+    if (N2 > 32) tmem_ld32(lane_addr + 32, c + 32);
+    const long long q = (tile - tk.block_begin) * kTcRows + tid;
+    if (q < tk.L * tk.R) {
+      const long long l = q % tk.L, r = q / tk.L;
+      float2* __restrict__ out = static_cast<float2*>(tk.out);
+      const long long obase = l + tk.L * (long long)Dout * r;
+#pragma unroll
+      for (int k = 0; k < kTcMaxD; ++k) {
+        if (k < Dout) {
+          const float im = (Dq == 8) ? c[8 + k] : (Dq == 16 ? c[16 + k] : (Dq == 24 ? c[24 + k] : c[32 + k]));
+          out[obase + tk.L * k] = make_float2(c[k], im);
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64u));
+  }
+}
+
+}  // namespace tnbp
