@@ -45,8 +45,12 @@ extern "C" {
 
 /* ---- precision of a job's device state ---- */
 #define TNBP_C128 0 /* plain path: complex128 storage and arithmetic */
-#define TNBP_C64 1  /* mixed path: complex64 storage, FP32 products, FP64 sums
-                       and FP64 truncation eigensolves */
+#define TNBP_C64 1  /* complex64 storage and BP sweeps (3xTF32 / FP32 products,
+                       FP64 sums), FP64 truncation eigensolves */
+#define TNBP_MIXED 2 /* mixed path: complex128 state (site tensors, messages),
+                        BP sweeps on a complex64 copy of the site tensors
+                        (3xTF32 / FP32 products, FP64 sums); AbsorbTPO,
+                        truncation and measurement in FP64 */
 
 typedef struct tnbp_job tnbp_job;
 typedef struct tnbp_tpo tnbp_tpo;
@@ -128,7 +132,7 @@ int tnbp_kicked_ising_tpo(const int32_t* edges, int64_t n_edges, double Jz, doub
 /* InitTensorProductState (include/tnbp/ptns/function/init.h:18-95): product
    state |0...0> (site tensors of shape (1,...,1,d) holding e_0), every
    message the 1x1 tensor [1].  phys_dims may be NULL (all 2).  precision is
-   TNBP_C128 or TNBP_C64.  stream is a cudaStream_t (NULL = a stream the job
+   TNBP_C128, TNBP_C64 or TNBP_MIXED.  stream is a cudaStream_t (NULL = a stream the job
    creates).  hbm_budget_bytes = 0 means no limit. */
 int tnbp_job_create(const int32_t* edges, int64_t n_edges, const int32_t* phys_dims,
                     int32_t precision, void* stream, uint64_t hbm_budget_bytes, tnbp_job** out);
@@ -175,11 +179,14 @@ int tnbp_bp_condition(tnbp_job* job, double* result);
    stop after the first whose condition is < tol.  Runs each sweep once
    (the condition of sweep k is the distance between sweep k+1 and sweep
    k, so the recomputation is shared).  iters_out = sweeps applied;
-   cond_out = last condition (NaN if max_iter == 0).  On a TNBP_C64 job the
-   tolerance used is max(tol, 1e-6) and the loop also stops at the first
-   sweep whose condition is larger than the previous one: the complex64
-   condition has a rounding floor near 1e-7, and sweeping past the minimum
-   only feeds unstable BP modes. */
+   cond_out = last condition (NaN if max_iter == 0).  On a TNBP_C64 or
+   TNBP_MIXED job the
+   tolerance used is max(tol, 1e-7) and, once the previous condition is
+   below 1e-5, the loop also stops at the first sweep whose condition is
+   larger than the previous one (keeping the messages before it): the
+   complex64 condition has a rounding floor near 1e-7, and sweeping past
+   the minimum only feeds unstable BP modes.  A non-finite condition fails
+   with TNBP_ENOTCONV. */
 int tnbp_bp_run(tnbp_job* job, double tol, int32_t max_iter, int32_t* iters_out,
                 double* cond_out);
 
@@ -275,7 +282,11 @@ int tnbp_server_submit_kicked_ising(tnbp_server* srv, int32_t L, int32_t chi, in
    number of requests that completed during this call. */
 int tnbp_server_step(tnbp_server* srv, int32_t* n_active_out, int32_t* n_queued_out,
                      int32_t* n_done_out);
-/* Result of a finished request: sum (re, im), 0 if done, 1 if pending. */
+/* Result of a finished request: sum (re, im); *pending_out = 0 if done, 1 if
+   pending.  A request whose own work failed (non-finite BP condition,
+   truncation error) is done and returns its error code (TNBP_ENOTCONV ...)
+   with the message in tnbp_last_error(); the other requests are unaffected.
+   A CUDA error fails tnbp_server_step itself. */
 int tnbp_server_result(tnbp_server* srv, int64_t request_id, double* sum_out,
                        int32_t* pending_out);
 

@@ -161,6 +161,32 @@ def test_end_to_end_estimator_matches_reference(name):
         assert abs(total - want) < 1e-12
 
 
+@pytest.mark.parametrize("name", ["ki3x3", "rc3x3", "chain6"])
+def test_mixed_path_estimator_within_1e6_of_reference(name):
+    """TNBP_MIXED (complex128 state, complex64 BP sweeps on 3xTF32 / FP32
+    products): every final expectation value of the estimator within 1e-6
+    of the reference's."""
+    R, meta = load_probe(os.path.join(HERE, "golden", f"probe_{name}.npz"))
+    src = open(os.path.join(HERE, "golden", "inputs", f"{name}.qasm")).read()
+    pauli = open(os.path.join(HERE, "golden", "inputs", f"{name}.txt")).read()
+    edges = tb.EdgesFromQasm(src)
+    layers = tb.QasmToTPO(src, edges)
+    with tb.State(edges, tb.MIXED) as st:
+        for layer in layers:
+            tb.AbsorbTPO(st, layer)
+            tb.BeliefPropagationLoop(st, meta["tol"], meta["maxit"])
+            tb.Truncation(st, meta["chi"], meta["sv_min"])
+        terms = tb.load_sparse_pauli(pauli, edges)
+        total, per = tb.MeasurePauliSum(st, terms)
+    ref_terms, _ = bn.parse_pauli_text(pauli, edges)
+    k1 = [i for i, t in enumerate(ref_terms) if t[0] == 1]
+    k2 = [i for i, t in enumerate(ref_terms) if t[0] == 2][: len(R["meas2/values"])]
+    for j, i in enumerate(k1):
+        assert abs(per[i] - R["meas1/values"][j]) < 1e-6
+    for j, i in enumerate(k2):
+        assert abs(per[i] - R["meas2/values"][j]) < 1e-6
+
+
 def _random_state(edges, rng, dims, d=2):
     """Random site tensors with the given bond dims and random Hermitian PSD
     messages (BP messages are of the form V (x)E V^H)."""
@@ -178,7 +204,7 @@ def _random_state(edges, rng, dims, d=2):
     return V, E
 
 
-@pytest.mark.parametrize("prec,atol", [(0, 1e-12), (1, 2e-5)])
+@pytest.mark.parametrize("prec,atol", [(0, 1e-12), (1, 2e-5), (2, 2e-5)])
 def test_random_uneven_sweep_condition_truncation(prec, atol):
     """Uneven bond dimensions in one launch: 3x4 lattice, dims 1..9."""
     rng = np.random.default_rng(11)
@@ -219,11 +245,41 @@ def test_large_bond_dims_sweep():
         F = bn.bp_sweep(edges, V, E)
         for m in range(2 * len(edges)):
             _close(st.get_message(m), F[m], 1e-12)
-    with tb.State(edges, tb.C64) as st:
+    for prec in (tb.C64, tb.MIXED):
+        with tb.State(edges, prec) as st:
+            st.set_state(V, E)
+            tb.BeliefPropagation(st)
+            for m in range(2 * len(edges)):
+                _close(st.get_message(m), F[m], 5e-5)
+
+
+def test_bond_dim_64_mixed_with_small_dims():
+    """D = 64 edges (chi = 32 during BP) next to D <= 32 edges on a 3x2 patch:
+    in complex64 one level then holds tcgen05 tasks and CUDA-core tasks;
+    complex128 truncation of the D = 64 messages to chi = 32."""
+    rng = np.random.default_rng(8)
+    edges = tb.bond_square_lattice(3, 2)
+    dims = [64 if m % 2 == 0 else 16 for m in range(len(edges))]
+    V, E = _random_state(edges, rng, dims)
+    F = bn.bp_sweep(edges, V, E)
+    with tb.State(edges, tb.C128) as st:
         st.set_state(V, E)
         tb.BeliefPropagation(st)
         for m in range(2 * len(edges)):
-            _close(st.get_message(m), F[m], 5e-5)
+            _close(st.get_message(m), F[m], 1e-12)
+        st.set_state(V, F)
+        d, e = tb.Truncation(st, 32, 1e-8)
+        Vt, Et, dr, er = bn.truncate(edges, V, F, 32, 1e-8)
+        assert list(d) == dr
+        _close(e, er, 1e-10)
+        for m in range(2 * len(edges)):
+            _close(st.get_message(m), Et[m], 1e-10)
+    for prec in (tb.C64, tb.MIXED):
+        with tb.State(edges, prec) as st:
+            st.set_state(V, E)
+            tb.BeliefPropagation(st)
+            for m in range(2 * len(edges)):
+                _close(st.get_message(m), F[m], 5e-5)
 
 
 def test_config1_kicked_ising_4x4():

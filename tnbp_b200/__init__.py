@@ -18,7 +18,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libtnbp_b200.so")
 
-C128, C64 = 0, 1
+C128, C64, MIXED = 0, 1, 2
 OK, EINVAL, ECUDA, ENOMEM, ENOTCONV, EPARSE, EUNSUPPORTED, ENOGPU = 0, -1, -2, -3, -4, -5, -6, -7
 
 

@@ -294,6 +294,7 @@ int tnbp_upload_message(tnbp_job* job, int64_t m, int32_t dim, const double* dat
       J.dim[m % ne] = dim;
       J.layout();
       J.V.alloc(J.v_elems * J.esz, J.stream);
+      J.shadow_dirty = true;
       J.M[0].alloc(J.m_elems * J.esz, J.stream);
       J.M[1].alloc(J.m_elems * J.esz, J.stream);
       for (size_t s = 0; s < oelems.size(); ++s)

@@ -132,13 +132,16 @@ int Graph::in_msg(int s, int k) const {
 Job::Job(const int32_t* e, int64_t n, const int32_t* pdims, int precision, cudaStream_t s,
          uint64_t budget)
     : g(e, n), prec(precision), budget(budget) {
-  if (precision != TNBP_C128 && precision != TNBP_C64) throw Error(TNBP_EINVAL, "unknown precision");
+  if (precision != TNBP_C128 && precision != TNBP_C64 && precision != TNBP_MIXED)
+    throw Error(TNBP_EINVAL, "unknown precision");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
     throw Error(TNBP_ENOGPU, "no CUDA device visible: the B200 engine has no CPU path");
   }
-  esz = prec == TNBP_C128 ? 16 : 8;
+  sprec = prec == TNBP_C64 ? TNBP_C64 : TNBP_C128;
+  esz = sprec == TNBP_C128 ? 16 : 8;
+  wsz = prec == TNBP_C128 ? 16 : 8;
   keep_pool_memory();
   if (s) {
     stream = s;
@@ -171,7 +174,7 @@ Job::Job(const int32_t* e, int64_t n, const int32_t* pdims, int precision, cudaS
 Job::~Job() {
   destroy_graphs();
   cudaStreamSynchronize(stream);
-  V.release(); M[0].release(); M[1].release();
+  V.release(); M[0].release(); M[1].release(); V32.release();
   plan = SweepPlan();
   if (host_scalar) cudaFreeHost(host_scalar);
   if (ev0) cudaEventDestroy(ev0);
@@ -211,7 +214,8 @@ void Job::layout() {
 
 void Job::put_complex(DevBuf& dst, const double* src, size_t n, size_t elem_off) {
   if (n == 0) return;
-  if (prec == TNBP_C128) {
+  if (&dst == &V) shadow_dirty = true;
+  if (sprec == TNBP_C128) {
     CK(cudaMemcpyAsync(static_cast<char*>(dst.p) + elem_off * 16, src, n * 16, cudaMemcpyHostToDevice, stream));
     CK(cudaStreamSynchronize(stream));
   } else {
@@ -223,7 +227,7 @@ void Job::put_complex(DevBuf& dst, const double* src, size_t n, size_t elem_off)
 }
 void Job::get_complex(const DevBuf& src, double* dst, size_t n, size_t elem_off) {
   if (n == 0) return;
-  if (prec == TNBP_C128) {
+  if (sprec == TNBP_C128) {
     CK(cudaMemcpyAsync(dst, static_cast<const char*>(src.p) + elem_off * 16, n * 16, cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
   } else {
@@ -235,7 +239,7 @@ void Job::get_complex(const DevBuf& src, double* dst, size_t n, size_t elem_off)
 }
 
 uint64_t Job::device_bytes() const {
-  return V.bytes + M[0].bytes + M[1].bytes + plan.bytes();
+  return V.bytes + M[0].bytes + M[1].bytes + V32.bytes + plan.bytes();
 }
 void Job::check_budget() const {
   if (budget && device_bytes() > budget)
@@ -244,6 +248,26 @@ void Job::check_budget() const {
 }
 
 void* Job::vptr(int s) const { return static_cast<char*>(V.p) + voff[s] * esz; }
+void* Job::sweep_vptr(int s) const {
+  return prec == TNBP_MIXED ? static_cast<char*>(V32.p) + voff[s] * 8 : vptr(s);
+}
+
+// TNBP_MIXED: round the complex128 site tensors to the complex64 copy that
+// the sweeps read.  A re-allocated copy invalidates the sweep plan (its
+// tasks and graphs hold the old addresses).
+void Job::sync_shadow() {
+  if (prec != TNBP_MIXED || !shadow_dirty) return;
+  if (!V32.p || V32.bytes != v_elems * 8) {
+    destroy_graphs();
+    plan = SweepPlan();
+    V32.alloc(v_elems * 8, stream);
+  }
+  const unsigned grid = (unsigned)std::min<size_t>((v_elems + 255) / 256, (size_t)8 * num_sms());
+  k_narrow<<<grid, 256, 0, stream>>>(static_cast<const double2*>(V.p), static_cast<float2*>(V32.p), v_elems);
+  CK(cudaGetLastError());
+  note_launch();
+  shadow_dirty = false;
+}
 void* Job::mptr(int arena, int m) const { return static_cast<char*>(M[arena].p) + moff[m] * esz; }
 
 void Job::destroy_graphs() {
@@ -359,10 +383,10 @@ void Job::build_plan() {
   std::vector<size_t> slot_base(ns, 0);
   size_t o = 0;
   for (int s = 0; s < ns; ++s) { slot_base[s] = o; o += (size_t)nslots[s] * align_elems(site_elems(s)); }
-  plan.scratch.alloc(std::max<size_t>(o, 32) * esz, stream);
+  plan.scratch.alloc(std::max<size_t>(o, 32) * wsz, stream);
   auto slot_ptr = [&](int s, int slot) -> void* {
-    if (slot < 0) return vptr(s);
-    return static_cast<char*>(plan.scratch.p) + (slot_base[s] + (size_t)slot * align_elems(site_elems(s))) * esz;
+    if (slot < 0) return sweep_vptr(s);
+    return static_cast<char*>(plan.scratch.p) + (slot_base[s] + (size_t)slot * align_elems(site_elems(s))) * wsz;
   };
   int maxlevel = 0;
   for (auto& op : ops) maxlevel = std::max(maxlevel, op.level + 1);
@@ -401,11 +425,11 @@ void Job::build_plan() {
     for (int k = 0; k < gs; ++k) sumD += sh[k];
     // algorithmic work of bp.h's schedule: 8 d prod(D) sum(D) flops per message
     plan.flops += gs * 8.0 * n * sumD;
-    plan.bytes_alg += n * esz;  // each site tensor read once
+    plan.bytes_alg += n * wsz;  // each site tensor read once (as the sweep reads it)
     for (int t = 0; t < gs; ++t) {
       GramTask g1;
       g1.A = slot_ptr(s, result[s][t]);
-      g1.B = vptr(s);
+      g1.B = sweep_vptr(s);
       long long L = 1, M = 1;
       for (int k = 0; k < t; ++k) L *= sh[k];
       for (size_t k = t + 1; k < sh.size(); ++k) M *= sh[k];
@@ -462,49 +486,45 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
     nlev = std::max(nlev, e.job->plan.levels.size());
   }
   b.levels.resize(nlev);
+  // The kernel is chosen per task, never per launch: complex64 tasks with
+  // Din, Dout <= 32 run on the tcgen05 kernel, every other task on the
+  // CUDA-core kernel, whatever else shares the batch.  A request's rounding
+  // therefore does not depend on what it is batched with.
+  const bool tc_ok = !entries.empty() && reduced_sweeps(entries[0].job->prec) && tcgen05_enabled();
   for (size_t lv = 0; lv < nlev; ++lv) {
-    std::vector<LegTask> t;
-    std::vector<long long> beg;
-    long long nb = 0;
+    std::vector<LegTask> t, t2;
+    std::vector<long long> beg, b2;
+    long long nb = 0, nb2 = 0;
     int maxdin = 1;
     for (auto& e : entries) {
       const auto& P = e.job->plan;
       if (lv >= P.levels.size()) continue;
       for (LegTask lt : P.levels[lv].tasks[e.parity]) {
-        lt.block_begin = nb;
-        beg.push_back(nb);
-        nb += (lt.L * lt.R + kRowTile - 1) / kRowTile;
-        t.push_back(lt);
+        if (tc_ok && lt.Din <= tc::kTcMaxD && lt.Dout <= tc::kTcMaxD) {
+          lt.block_begin = nb2;
+          b2.push_back(nb2);
+          nb2 += (lt.L * lt.R + tc::kTcRows - 1) / tc::kTcRows;
+          t2.push_back(lt);
+        } else {
+          lt.block_begin = nb;
+          beg.push_back(nb);
+          nb += (lt.L * lt.R + kRowTile - 1) / kRowTile;
+          maxdin = std::max(maxdin, lt.Din);
+          t.push_back(lt);
+        }
       }
-      maxdin = std::max(maxdin, P.levels[lv].max_din);
     }
-    upload_vec(b.levels[lv].tasks, t, stream);
-    upload_vec(b.levels[lv].begins, beg, stream);
-    b.levels[lv].ntask = (int)t.size();
-    b.levels[lv].nblocks = nb;
-    b.levels[lv].max_din = maxdin;
-    // complex64 levels whose dims fit the tcgen05 kernel run on the tensor cores
-    int maxdout = 1;
-    for (auto& lt : t) maxdout = std::max(maxdout, lt.Dout);
-    if (!entries.empty() && entries[0].job->prec == TNBP_C64 && tcgen05_enabled() && maxdin <= tc::kTcMaxD &&
-        maxdout <= tc::kTcMaxD && !t.empty()) {
-      std::vector<LegTask> t2 = t;
-      std::vector<long long> b2;
-      long long nb2 = 0;
-      int dp = 4, dq = 8;
-      for (auto& lt : t2) {
-        lt.block_begin = nb2;
-        b2.push_back(nb2);
-        nb2 += (lt.L * lt.R + tc::kTcRows - 1) / tc::kTcRows;
-        dp = std::max(dp, (lt.Din + 3) & ~3);
-        dq = std::max(dq, (lt.Dout + 7) & ~7);
-      }
-      upload_vec(b.levels[lv].tc_tasks, t2, stream);
-      upload_vec(b.levels[lv].tc_begins, b2, stream);
-      b.levels[lv].tc_nblocks = nb2;
-      b.levels[lv].tc_smem = tc::leg_smem_bytes();
-      b.levels[lv].use_tc = true;
-    }
+    SweepBatch::Level& L = b.levels[lv];
+    upload_vec(L.tasks, t, stream);
+    upload_vec(L.begins, beg, stream);
+    L.ntask = (int)t.size();
+    L.nblocks = nb;
+    L.max_din = maxdin;
+    upload_vec(L.tc_tasks, t2, stream);
+    upload_vec(L.tc_begins, b2, stream);
+    L.tc_ntask = (int)t2.size();
+    L.tc_nblocks = nb2;
+    L.tc_smem = tc::leg_smem_bytes();
   }
   std::vector<GramTask> gt;
   std::vector<long long> gb;
@@ -547,32 +567,31 @@ static size_t leg_smem(int max_din) {
 
 // Largest dynamic shared memory any leg-apply launch may ask for; set once
 // per process outside of stream capture.
-template <typename R>
+template <typename R, typename MR>
 static void leg_apply_attr() {
   static bool done = false;
   if (done) return;
-  CK(cudaFuncSetAttribute(k_leg_apply<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)leg_smem<R>(128)));
+  CK(cudaFuncSetAttribute(k_leg_apply<R, MR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)leg_smem<R>(128)));
   done = true;
 }
 
-template <typename R>
+template <typename R, typename MR>
 static int launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
   int n = 0;
   for (auto& lv : b.levels) {
-    if (lv.ntask == 0) continue;
-    if (lv.use_tc) {
+    if (lv.tc_ntask > 0) {
       // persistent: up to 2 CTAs per SM, each over a contiguous range of tiles
       const long long grid = std::min<long long>(lv.tc_nblocks, 2LL * num_sms());
-      k_leg_apply_tc<<<(unsigned)grid, 128, lv.tc_smem, stream>>>(
-          static_cast<const LegTask*>(lv.tc_tasks.p), static_cast<const long long*>(lv.tc_begins.p), lv.ntask,
+      k_leg_apply_tc<MR><<<(unsigned)grid, 128, lv.tc_smem, stream>>>(
+          static_cast<const LegTask*>(lv.tc_tasks.p), static_cast<const long long*>(lv.tc_begins.p), lv.tc_ntask,
           lv.tc_nblocks);
       CK(cudaGetLastError());
       ++n;
-      continue;
     }
+    if (lv.ntask == 0) continue;
     if (lv.max_din > 128) throw Error(TNBP_EUNSUPPORTED, "bond dimension above 128 during BP");
     const size_t smem = leg_smem<R>(lv.max_din);
-    k_leg_apply<R><<<(unsigned)lv.nblocks, kThreads, smem, stream>>>(
+    k_leg_apply<R, MR><<<(unsigned)lv.nblocks, kThreads, smem, stream>>>(
         static_cast<const LegTask*>(lv.tasks.p), static_cast<const long long*>(lv.begins.p), lv.ntask, lv.max_din);
     CK(cudaGetLastError());
     ++n;
@@ -581,7 +600,7 @@ static int launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
     k_gram<R><<<(unsigned)b.gram_nblocks, kThreads, 0, stream>>>(
         static_cast<const GramTask*>(b.gram_tasks.p), static_cast<const long long*>(b.gram_begins.p), b.gram_ntask);
     CK(cudaGetLastError());
-    k_msg_finalize<R><<<b.nmsg, kThreads, 0, stream>>>(static_cast<const MsgTask*>(b.msg_tasks.p));
+    k_msg_finalize<R, MR><<<b.nmsg, kThreads, 0, stream>>>(static_cast<const MsgTask*>(b.msg_tasks.p));
     CK(cudaGetLastError());
     n += 2;
   }
@@ -593,21 +612,32 @@ static int launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
   return n;
 }
 
+// Sweep kernels: TNBP_C128 all complex128; TNBP_C64 all complex64;
+// TNBP_MIXED complex64 tensors with complex128 messages.
 int launch_batch(const SweepBatch& b, int prec, cudaStream_t stream) {
-  return prec == TNBP_C128 ? launch_batch_t<double>(b, stream) : launch_batch_t<float>(b, stream);
+  if (prec == TNBP_C128) return launch_batch_t<double, double>(b, stream);
+  if (prec == TNBP_C64) return launch_batch_t<float, float>(b, stream);
+  return launch_batch_t<float, double>(b, stream);
+}
+
+template <typename MR>
+static void tc_attr() {
+  static bool done = false;
+  if (done) return;
+  CK(cudaFuncSetAttribute(k_leg_apply_tc<MR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)tc::leg_smem_bytes()));
+  done = true;
 }
 
 void prepare_kernels(int prec) {
   if (prec == TNBP_C128) {
-    leg_apply_attr<double>();
+    leg_apply_attr<double, double>();
+  } else if (prec == TNBP_C64) {
+    leg_apply_attr<float, float>();
+    tc_attr<float>();
   } else {
-    leg_apply_attr<float>();
-    static bool tc_done = false;
-    if (!tc_done) {
-      CK(cudaFuncSetAttribute(k_leg_apply_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)tc::leg_smem_bytes()));
-      tc_done = true;
-    }
+    leg_apply_attr<float, double>();
+    tc_attr<double>();
   }
 }
 
@@ -646,6 +676,7 @@ void check_tc_error(cudaStream_t stream) {
 }
 
 void Job::run_sweep(int par) {
+  sync_shadow();
   if (!plan.valid) build_plan();
   SweepBatch& b = plan.single[par];
   if (!b.graph) {
@@ -673,7 +704,7 @@ void Job::run_sweep(int par) {
 double Job::read_cond() {
   CK(cudaMemcpyAsync(host_scalar, plan.single[last_par].cond.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
-  if (prec == TNBP_C64) check_tc_error(stream);
+  if (reduced_sweeps(prec)) check_tc_error(stream);
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) {
     last_sweep_ms = ms;
@@ -688,7 +719,7 @@ void Job::bp_sweep() {
   run_sweep(cur);
   cur = 1 - cur;
   CK(cudaStreamSynchronize(stream));
-  if (prec == TNBP_C64) check_tc_error(stream);
+  if (reduced_sweeps(prec)) check_tc_error(stream);
 }
 
 double Job::bp_condition() {
@@ -700,15 +731,22 @@ double Job::bp_condition() {
 // (about 1e-7 per sweep for normalized messages); a tolerance under the
 // floor would run every sweep to max_iter and let unstable BP modes grow
 // from rounding noise.  The mixed path therefore stops at
-// max(tol, kC64TolFloor).
+// max(tol, kC64TolFloor) (1e-7: a floor of 1e-6 left the messages about
+// 1e-6 from the fixed point and the expectation values as far from the
+// plain path's).
 double effective_tol(int prec, double tol) {
-  return prec == TNBP_C64 ? std::max(tol, kC64TolFloor) : tol;
+  return reduced_sweeps(prec) ? std::max(tol, kC64TolFloor) : tol;
 }
 
-// The mixed path also stops as soon as the condition grows: past the
-// minimum the unstable BP mode amplifies rounding noise every sweep (the
-// plain path keeps the reference's rule exactly).
-bool stop_on_growth(int prec) { return prec == TNBP_C64; }
+// The mixed path also stops when the condition grows once it is within two
+// decades of its rounding floor (prev < kC64GrowthGate): past the minimum
+// the unstable BP mode amplifies rounding noise every sweep.  Growth at
+// larger conditions is ordinary BP dynamics, which the plain path sees too,
+// and does not stop the loop.  The plain path keeps the reference's rule
+// exactly.
+bool stop_on_growth(int prec, double prev, double c) {
+  return reduced_sweeps(prec) && prev < kC64GrowthGate && c > prev;
+}
 
 void Job::bp_run(double tol_in, int max_iter, int* iters, double* cond) {
   const double tol = effective_tol(prec, tol_in);
@@ -723,9 +761,10 @@ void Job::bp_run(double tol_in, int max_iter, int* iters, double* cond) {
     run_sweep(cur);
     const double c = read_cond();
     *cond = c;
+    if (!std::isfinite(c)) throw Error(TNBP_ENOTCONV, "BP condition is not finite (non-finite messages)");
     if (c < tol) break;
     if (*iters >= max_iter) break;
-    if (stop_on_growth(prec) && c > prev) break;
+    if (stop_on_growth(prec, prev, c)) break;
     prev = c;
     cur = 1 - cur;
     ++*iters;
@@ -736,6 +775,7 @@ void Job::bp_run(double tol_in, int max_iter, int* iters, double* cond) {
 Tpo::~Tpo() {}
 
 void Job::absorb_tpo(const Tpo& tpo) {
+  shadow_dirty = true;
   const int ns = (int)g.labels.size();
   const int ne = (int)g.edges.size();
   if ((int)tpo.rank.size() != ne) throw Error(TNBP_EINVAL, "TPO edge count mismatch");
@@ -788,7 +828,7 @@ void Job::absorb_tpo(const Tpo& tpo) {
   upload_vec(dab, ab, stream);
   upload_vec(dmt, mt, stream);
   upload_vec(dmb, mb, stream);
-  if (prec == TNBP_C128) {
+  if (sprec == TNBP_C128) {
     (k_absorb_sites<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<AbsorbTask*>(dat.p), static_cast<long long*>(dab.p), (int)at.size()), note_launch());
     (k_expand_msgs<double><<<(unsigned)nmb, kThreads, 0, stream>>>(static_cast<MsgExpandTask*>(dmt.p), static_cast<long long*>(dmb.p), (int)mt.size()), note_launch());
   } else {
@@ -869,8 +909,8 @@ void Job::run_chains(std::vector<ChainEntry>& chains) {
     upload_vec(dt, t, stream);
     upload_vec(db, b, stream);
     if (maxdin > 128) throw Error(TNBP_EUNSUPPORTED, "bond dimension above 128");
-    prepare_kernels(prec);
-    if (prec == TNBP_C128) {
+    prepare_kernels(sprec);
+    if (sprec == TNBP_C128) {
       const size_t smem = leg_smem<double>(maxdin);
       (k_leg_apply<double><<<(unsigned)nb, kThreads, smem, stream>>>(static_cast<LegTask*>(dt.p), static_cast<long long*>(db.p), (int)t.size(), maxdin), note_launch());
     } else {
@@ -884,6 +924,7 @@ void Job::run_chains(std::vector<ChainEntry>& chains) {
 
 // --------------------------------------------------------------- truncation
 void Job::truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_out) {
+  shadow_dirty = true;
   if (chi_max < 1) throw Error(TNBP_EINVAL, "chi_max must be >= 1");
   const int ns = (int)g.labels.size();
   const int ne = (int)g.edges.size();
@@ -924,7 +965,7 @@ void Job::truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_ou
   }
   DevBuf dtt;
   upload_vec(dtt, tt, stream);
-  if (prec == TNBP_C128) (k_truncate_edges<double><<<ne, kThreads, 0, stream>>>(static_cast<TruncTask*>(dtt.p), chi_max, sv_min), note_launch());
+  if (sprec == TNBP_C128) (k_truncate_edges<double><<<ne, kThreads, 0, stream>>>(static_cast<TruncTask*>(dtt.p), chi_max, sv_min), note_launch());
   else (k_truncate_edges<float><<<ne, kThreads, 0, stream>>>(static_cast<TruncTask*>(dtt.p), chi_max, sv_min), note_launch());
   CK(cudaGetLastError());
   std::vector<int> hkeep(ne), hstatus(ne);
@@ -979,7 +1020,7 @@ void Job::truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_ou
   }
   DevBuf ddt;
   upload_vec(ddt, dt, stream);
-  if (prec == TNBP_C128) (k_write_diag<double><<<2 * ne, 128, 0, stream>>>(static_cast<DiagTask*>(ddt.p)), note_launch());
+  if (sprec == TNBP_C128) (k_write_diag<double><<<2 * ne, 128, 0, stream>>>(static_cast<DiagTask*>(ddt.p)), note_launch());
   else (k_write_diag<float><<<2 * ne, 128, 0, stream>>>(static_cast<DiagTask*>(ddt.p)), note_launch());
   CK(cudaGetLastError());
   std::swap(M[0], nM0);
@@ -991,13 +1032,19 @@ void Job::truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_ou
   CK(cudaStreamSynchronize(stream));
   if (dims_out) for (int e = 0; e < ne; ++e) dims_out[e] = hkeep[e];
   if (err_out) for (int e = 0; e < ne; ++e) err_out[e] = herr[e];
-  int bad = 0;
-  for (int e = 0; e < ne; ++e) bad += hstatus[e] != 0;
+  int bad = 0, nonfinite = 0;
+  for (int e = 0; e < ne; ++e) {
+    bad += hstatus[e] == 1;
+    nonfinite += hstatus[e] == 2;
+  }
+  if (nonfinite)
+    throw Error(TNBP_ENOTCONV, std::to_string(nonfinite) + " edge(s) with non-finite messages at truncation");
   if (bad) throw Error(TNBP_ENOTCONV, std::to_string(bad) + " edge SVD(s) reached the Jacobi sweep limit");
   check_budget();
 }
 
 void Job::normalize_sites() {
+  shadow_dirty = true;
   const int ns = (int)g.labels.size();
   const int per_thread = 8;
   std::vector<RangeTask> rt;
@@ -1022,7 +1069,7 @@ void Job::normalize_sites() {
   DevBuf drt, drb;
   upload_vec(drt, rt, stream);
   upload_vec(drb, rb, stream);
-  if (prec == TNBP_C128) {
+  if (sprec == TNBP_C128) {
     (k_sumsq_partial<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<RangeTask*>(drt.p), static_cast<long long*>(drb.p), ns, per_thread), note_launch());
     (k_scale_ranges<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<RangeTask*>(drt.p), static_cast<long long*>(drb.p), ns, per_thread), note_launch());
   } else {
@@ -1132,7 +1179,7 @@ void Job::compute_envs(const std::vector<int>& sites1, const std::vector<std::pa
   upload_vec(dgb, gb, stream);
   upload_vec(dpt, pt, stream);
   if (!gt.empty()) {
-    if (prec == TNBP_C128) (k_gram<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<GramTask*>(dgt.p), static_cast<long long*>(dgb.p), (int)gt.size()), note_launch());
+    if (sprec == TNBP_C128) (k_gram<double><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<GramTask*>(dgt.p), static_cast<long long*>(dgb.p), (int)gt.size()), note_launch());
     else (k_gram<float><<<(unsigned)nb, kThreads, 0, stream>>>(static_cast<GramTask*>(dgt.p), static_cast<long long*>(dgb.p), (int)gt.size()), note_launch());
     CK(cudaGetLastError());
     (k_partial_sum<<<(unsigned)pt.size(), kThreads, 0, stream>>>(static_cast<PartialSumTask*>(dpt.p)), note_launch());

@@ -74,9 +74,10 @@ struct SweepBatch {
     int ntask = 0;
     long long nblocks = 0;
     int max_din = 1;
-    // tcgen05 path (complex64, all dims <= 32): 128-row tiles
-    bool use_tc = false;
+    // tasks of the tcgen05 kernel (complex64, Din and Dout <= 32): 128-row
+    // tiles; the fields above hold the level's other tasks
     DevBuf tc_tasks, tc_begins;
+    int tc_ntask = 0;
     long long tc_nblocks = 0;
     size_t tc_smem = 0;
   };
@@ -118,9 +119,11 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
 int launch_batch(const SweepBatch& b, int prec, cudaStream_t stream);
 void note_launch(int n = 1);
 void keep_pool_memory();
-constexpr double kC64TolFloor = 1e-6;
+constexpr double kC64TolFloor = 1e-7;
+constexpr double kC64GrowthGate = 1e-5;
 double effective_tol(int prec, double tol);
-bool stop_on_growth(int prec);
+bool stop_on_growth(int prec, double prev, double c);
+inline bool reduced_sweeps(int prec) { return prec != TNBP_C128; }
 void prepare_kernels(int prec);
 bool tcgen05_enabled();
 int num_sms();
@@ -149,8 +152,10 @@ struct ChainEntry;
 
 struct Job {
   Graph g;
-  int prec;
-  size_t esz;
+  int prec;      // TNBP_C128, TNBP_C64 or TNBP_MIXED
+  int sprec;     // storage precision: TNBP_C64 for TNBP_C64, else TNBP_C128
+  size_t esz;    // bytes of a stored complex element
+  size_t wsz;    // bytes of a complex element inside a BP sweep
   uint64_t budget;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -160,6 +165,10 @@ struct Job {
   std::vector<size_t> voff, moff;
   size_t v_elems = 0, m_elems = 0;
   DevBuf V, M[2];
+  // TNBP_MIXED: complex64 copy of V read by the BP sweeps, refreshed before
+  // the first sweep after V changed
+  DevBuf V32;
+  bool shadow_dirty = true;
   int cur = 0;
   int last_par = 0;
   SweepPlan plan;
@@ -178,6 +187,8 @@ struct Job {
   uint64_t device_bytes() const;
   void check_budget() const;
   void* vptr(int s) const;
+  void* sweep_vptr(int s) const;
+  void sync_shadow();
   void* mptr(int arena, int m) const;
   void destroy_graphs();
   void build_plan();

@@ -42,11 +42,15 @@ __device__ __forceinline__ int find_task(const long long* begins, int n, long lo
   return lo;
 }
 
-template <typename R>
+// R: arithmetic and tensor element type; MR: element type of mat (a message
+// or projector), which may be wider than R (complex128 messages of the mixed
+// path, rounded to R in shared memory).
+template <typename R, typename MR = R>
 __global__ void __launch_bounds__(kThreads) k_leg_apply(const LegTask* __restrict__ tasks,
                                                         const long long* __restrict__ begins,
                                                         int ntask, int max_din) {
   using C = typename cvec<R>::type;
+  using CM = typename cvec<MR>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ti = find_task(begins, ntask, blockIdx.x);
   const LegTask tk = tasks[ti];
@@ -59,7 +63,7 @@ __global__ void __launch_bounds__(kThreads) k_leg_apply(const LegTask* __restric
   C* Ms = As + kRowTile * (max_din + 1);               // [Din][33]
   const C* in = static_cast<const C*>(tk.in);
   C* out = static_cast<C*>(tk.out);
-  const C* mat = static_cast<const C*>(tk.mat);
+  const CM* mat = static_cast<const CM*>(tk.mat);
   const long long L = tk.L;
   const bool qfast = L >= kRowTile;
 
@@ -82,7 +86,7 @@ __global__ void __launch_bounds__(kThreads) k_leg_apply(const LegTask* __restric
     __syncthreads();
     for (int idx = threadIdx.x; idx < Din * kColTile; idx += kThreads) {
       const int kk = idx % kColTile, j = idx / kColTile;
-      Ms[j * (kColTile + 1) + kk] = kk < kc ? mat[j + (long long)Din * (k0 + kk)] : czero<C>();
+      Ms[j * (kColTile + 1) + kk] = kk < kc ? from_d2<C>(to_d2(mat[j + (long long)Din * (k0 + kk)])) : czero<C>();
     }
     __syncthreads();
 #pragma unroll
@@ -145,9 +149,14 @@ __global__ void __launch_bounds__(kThreads) k_gram(const GramTask* __restrict__ 
   const C* B = static_cast<const C*>(tk.B);
   const long long L = tk.L, LD = tk.L * tk.D, LDM = tk.L * tk.D * tk.M;
   const bool qfast = L >= kRowTile;
+  // complex64: each 32-row tile is summed in FP32 and added to an FP64
+  // accumulator, so rounding does not grow with the chunk length (up to 4096
+  // rows); complex128 accumulates directly.
+  constexpr bool kPromote = sizeof(R) == 4;
   C acc[4];
+  double2 accd[4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) acc[i] = czero<C>();
+  for (int i = 0; i < 4; ++i) { acc[i] = czero<C>(); accd[i] = make_double2(0.0, 0.0); }
   for (long long q0 = qbeg; q0 < qend; q0 += kRowTile) {
     __syncthreads();
     for (int idx = threadIdx.x; idx < kRowTile * kColTile; idx += kThreads) {
@@ -173,6 +182,12 @@ __global__ void __launch_bounds__(kThreads) k_gram(const GramTask* __restrict__ 
       const int a = o % kColTile, bb = o / kColTile;
 #pragma unroll 8
       for (int qq = 0; qq < kRowTile; ++qq) cfma_conj(acc[i], As[qq][a], Bs[qq][bb]);
+      if (kPromote) {
+        const double2 t = to_d2(acc[i]);
+        accd[i].x += t.x;
+        accd[i].y += t.y;
+        acc[i] = czero<C>();
+      }
     }
   }
   double2* part = tk.partial + (long long)chunk * tk.C * tk.C;
@@ -180,7 +195,7 @@ __global__ void __launch_bounds__(kThreads) k_gram(const GramTask* __restrict__ 
   for (int i = 0; i < 4; ++i) {
     const int o = threadIdx.x + i * kThreads;
     const int a = ca0 + o % kColTile, bb = cb0 + o / kColTile;
-    if (a < tk.C && bb < tk.C) part[a + (long long)tk.C * bb] = to_d2(acc[i]);
+    if (a < tk.C && bb < tk.C) part[a + (long long)tk.C * bb] = kPromote ? accd[i] : to_d2(acc[i]);
   }
 }
 
@@ -214,9 +229,10 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return red[0];
 }
 
-template <typename R>
+// OR: element type of the stored messages (out and old).
+template <typename R, typename OR = R>
 __global__ void __launch_bounds__(kThreads) k_msg_finalize(const MsgTask* __restrict__ tasks) {
-  using C = typename cvec<R>::type;
+  using C = typename cvec<OR>::type;
   __shared__ double red[32];
   const MsgTask tk = tasks[blockIdx.x];
   const int n = tk.C * tk.C;
@@ -245,6 +261,15 @@ __global__ void __launch_bounds__(kThreads) k_msg_finalize(const MsgTask* __rest
   if (threadIdx.x == 0) {
     if (tk.dist) *tk.dist = sqrt(d2);
     if (tk.norm_out) *tk.norm_out = nn;
+  }
+}
+
+// complex128 -> complex64 copy (round to nearest): the sweep copy of the
+// mixed path's site tensors.
+static __global__ void k_narrow(const double2* __restrict__ in, float2* __restrict__ out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 v = in[i];
+    out[i] = make_float2((float)v.x, (float)v.y);
   }
 }
 

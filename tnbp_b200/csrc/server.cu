@@ -29,7 +29,8 @@ namespace tnbp {
 
 Server::Server(int precision, uint64_t budget_bytes, int max_active_jobs)
     : prec(precision), budget(budget_bytes), max_active(max_active_jobs) {
-  if (precision != TNBP_C128 && precision != TNBP_C64) throw Error(TNBP_EINVAL, "unknown precision");
+  if (precision != TNBP_C128 && precision != TNBP_C64 && precision != TNBP_MIXED)
+    throw Error(TNBP_EINVAL, "unknown precision");
   if (max_active < 1) throw Error(TNBP_EINVAL, "max_active must be >= 1");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -55,10 +56,13 @@ Server::~Server() {
 
 // Peak device bytes of a kicked-Ising request on an L x L lattice: BP runs
 // at bond dimension 2*chi; per site the tensor, its copy during absorption
-// and truncation, and the sweep scratch slots of its degree; both message
-// arenas twice; per-edge truncation work.
+// and truncation, the complex64 sweep copy (TNBP_MIXED) and the sweep
+// scratch slots of its degree; both message arenas twice; per-edge
+// truncation work.
 uint64_t Server::footprint(const Request& r) const {
-  const double esz = prec == TNBP_C128 ? 16.0 : 8.0;
+  const double esz = prec == TNBP_C64 ? 8.0 : 16.0;   // stored element
+  const double wsz = prec == TNBP_C128 ? 16.0 : 8.0;  // sweep element
+  const double shadow = prec == TNBP_MIXED ? 8.0 : 0.0;
   const double D = 2.0 * r.chi;
   const int L = r.L;
   double bytes = 0.0;
@@ -67,7 +71,7 @@ uint64_t Server::footprint(const Request& r) const {
       const int g = (x > 0) + (x < L - 1) + (y > 0) + (y < L - 1);
       const int slots = g == 4 ? 8 : g == 3 ? 5 : g == 2 ? 2 : 0;
       const double n = 2.0 * std::pow(D, g);
-      bytes += n * esz * (2.0 + slots);
+      bytes += n * (2.0 * esz + shadow + wsz * slots);
     }
   const double ne = 2.0 * L * (L - 1);
   bytes += 4.0 * 2.0 * ne * D * D * esz;      // message arenas (old + new)
@@ -145,6 +149,18 @@ void Server::finish(Request& r) {
   r.phase = Request::DONE;
 }
 
+// A request whose own work raises an error (a non-finite BP condition, a
+// truncation that reports non-finite messages or an SVD sweep limit) is
+// finished with that error; the other requests are not affected.
+void Server::fail(Request& r, int code, const std::string& msg) {
+  r.error_code = code;
+  r.error = msg;
+  r.result[0] = r.result[1] = std::nan("");
+  r.job.reset();
+  r.tpo.reset();
+  r.phase = Request::DONE;
+}
+
 void Server::step(int* n_active, int* n_queued, int* n_done) {
   int done = 0;
   // 1. admission by HBM footprint and free slots
@@ -178,7 +194,10 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
     }
   }
   if (!entries.empty()) {
-    for (auto* r : inbp) if (!r->job->plan.valid) r->job->build_plan();
+    for (auto* r : inbp) {
+      r->job->sync_shadow();
+      if (!r->job->plan.valid) r->job->build_plan();
+    }
     prepare_kernels(prec);
     build_batch(entries, batch, stream);
     note_launch(launch_batch(batch, prec, stream));
@@ -189,7 +208,7 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
     }
     CK(cudaMemcpyAsync(hcond, batch.cond.p, entries.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
-    if (prec == TNBP_C64) check_tc_error(stream);
+    if (reduced_sweeps(prec)) check_tc_error(stream);
     for (size_t i = 0; i < inbp.size(); ++i) {
       Request& r = *inbp[i];
       Job& j = *r.job;
@@ -199,7 +218,11 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
         continue;
       }
       const double c = hcond[i];
-      if (c < effective_tol(prec, r.tol) || r.bp_iters >= r.maxit || (stop_on_growth(prec) && c > r.prev_cond)) {
+      if (!std::isfinite(c)) {
+        fail(r, TNBP_ENOTCONV, "BP condition is not finite (non-finite messages)");
+        continue;
+      }
+      if (c < effective_tol(prec, r.tol) || r.bp_iters >= r.maxit || stop_on_growth(prec, r.prev_cond, c)) {
         r.phase = Request::TRUNC;  // keep the current messages
       } else {
         r.prev_cond = c;
@@ -211,13 +234,18 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
   // 4. truncation, next step or measurement
   for (int64_t id : active) {
     Request& r = *reqs[id];
-    if (r.phase == Request::TRUNC) {
-      r.job->truncate(r.chi, r.sv_min, nullptr, nullptr);
-      ++r.step;
-      r.phase = r.step < r.steps ? Request::ABSORB : Request::MEASURE;
+    try {
+      if (r.phase == Request::TRUNC) {
+        r.job->truncate(r.chi, r.sv_min, nullptr, nullptr);
+        ++r.step;
+        r.phase = r.step < r.steps ? Request::ABSORB : Request::MEASURE;
+      }
+      if (r.phase == Request::MEASURE) finish(r);
+    } catch (const Error& e) {
+      if (e.code == TNBP_ECUDA) throw;  // the device context is not usable
+      fail(r, e.code, e.what());
     }
-    if (r.phase == Request::MEASURE) {
-      finish(r);
+    if (r.phase == Request::DONE) {
       in_use -= r.footprint;
       ++done;
     }
@@ -309,6 +337,7 @@ int tnbp_server_result(tnbp_server* srv, int64_t id, double* sum, int32_t* pendi
     if (it == srv->s->reqs.end()) throw tnbp::Error(TNBP_EINVAL, "unknown request id");
     const bool done = it->second->phase == tnbp::Request::DONE;
     if (pending) *pending = done ? 0 : 1;
+    if (done && it->second->error_code) throw tnbp::Error(it->second->error_code, it->second->error);
     if (sum && done) { sum[0] = it->second->result[0]; sum[1] = it->second->result[1]; }
   });
 }

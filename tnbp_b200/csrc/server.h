@@ -28,6 +28,8 @@ struct Request {
   double prev_cond = 0;
   uint64_t footprint = 0;
   double result[2] = {0, 0};
+  int error_code = 0;  // a request that failed keeps its error; others go on
+  std::string error;
 };
 
 struct Server {
@@ -51,6 +53,7 @@ struct Server {
   uint64_t footprint(const Request& r) const;
   void start(Request& r);
   void finish(Request& r);
+  void fail(Request& r, int code, const std::string& msg);
 };
 
 }  // namespace tnbp

@@ -1,5 +1,6 @@
 // Leg contraction on the 5th-generation tensor cores (tcgen05, sm_100a) for
-// the complex64 path:  out[l, k, r] = sum_j in[l, j, r] * M[j, k].
+// the complex64 and mixed paths:  out[l, k, r] = sum_j in[l, j, r] * M[j, k]
+// (in, out complex64; M complex64 or complex128).
 //
 // A CTA (128 threads) works through 128-row tiles, rows q = l + L*r.  The complex
 // product is one real GEMM
@@ -114,6 +115,7 @@ __host__ __device__ constexpr size_t leg_smem_bytes() {
 // task, and the next tile's global loads are issued before waiting for the
 // current tile's MMAs so that loads, tensor-core work and the epilogue
 // overlap.
+template <typename MR>
 __global__ void __launch_bounds__(128) k_leg_apply_tc(const LegTask* __restrict__ tasks,
                                                       const long long* __restrict__ begins, int ntask,
                                                       long long total_tiles) {
@@ -181,18 +183,20 @@ __global__ void __launch_bounds__(128) k_leg_apply_tc(const LegTask* __restrict_
       Dp = (Din + 3) & ~3;
       Dq = (Dout + 7) & ~7;
       const int K2 = 2 * Dp, N2 = 2 * Dq;
-      const float2* __restrict__ mat = static_cast<const float2*>(tk.mat);
+      const typename cvec<MR>::type* __restrict__ mat = static_cast<const typename cvec<MR>::type*>(tk.mat);
       // B_real[k2][n2] = [[M_re, M_im], [-M_im, M_re]], stored N2 x K2 K-major
       for (int n2 = warp; n2 < N2; n2 += 4) {
         const int nr = n2 < Dq ? n2 : n2 - Dq, pn = n2 < Dq ? 0 : 1;
         for (int k2 = tid & 31; k2 < K2; k2 += 32) {
           const int kr = k2 < Dp ? k2 : k2 - Dp, pk = k2 < Dp ? 0 : 1;
-          float v = 0.f;
+          double v = 0.0;
           if (kr < Din && nr < Dout) {
-            const float2 m = __ldg(&mat[kr + (long long)Din * nr]);
+            const double2 m = to_d2(mat[kr + (long long)Din * nr]);
             v = (pk == pn) ? m.x : (pk == 0 ? m.y : -m.y);
           }
-          const float h = to_tf32(v), lo = to_tf32(v - h);
+          // hi = tf32(v); lo = tf32 of the remainder, taken in FP64 so that
+          // complex128 messages keep their low bits
+          const float h = to_tf32((float)v), lo = to_tf32((float)(v - (double)h));
           *reinterpret_cast<float*>(b_hi + kmajor_off(n2, k2, N2)) = h;
           *reinterpret_cast<float*>(b_lo + kmajor_off(n2, k2, N2)) = lo;
         }

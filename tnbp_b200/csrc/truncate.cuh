@@ -30,7 +30,7 @@ struct TruncTask {
   double* s_keep;   // D: kept singular values of T
   int* keep_out;
   double* err_out;
-  int* status;      // 0 ok, 1 SVD sweep limit reached
+  int* status;      // 0 ok, 1 SVD sweep limit reached, 2 non-finite values
 };
 
 __device__ __forceinline__ double2 warp_sum2(double2 v) {
@@ -129,12 +129,16 @@ __device__ void block_sv_sort(const double2* A, int n, double* s_tmp, double* s,
     if (lane == 0) s_tmp[c] = sqrt(acc);
   }
   __syncthreads();
+  // Non-finite values (from non-finite messages) sort last as -1, so that
+  // the ranks stay a permutation and every perm[] entry is a valid column;
+  // the caller reports them.
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const double si = s_tmp[i];
+    const double ki = isfinite(si) ? si : -1.0;
     int rank = 0;
     for (int j = 0; j < n; ++j) {
-      const double sj = s_tmp[j];
-      rank += (sj > si) || (sj == si && j < i);
+      const double kj = isfinite(s_tmp[j]) ? s_tmp[j] : -1.0;
+      rank += (kj > ki) || (kj == ki && j < i);
     }
     s[rank] = si;
     perm[rank] = i;
@@ -214,6 +218,8 @@ __global__ void __launch_bounds__(kThreads) k_truncate_edges(const TruncTask* __
   int* pT = tk.perm + 2 * n;
   if (block_jacobi(W0, W1, n, &flag, red) < 0 && threadIdx.x == 0) *tk.status = 1;
   block_sv_sort(W0, n, s_tmp, sT, pT);
+  for (int k = threadIdx.x; k < 3 * n; k += kThreads)
+    if (!isfinite(tk.sv[k])) *tk.status = 2;  // non-finite message or T
   int keep = 0;
   while (keep < n && keep < chi_max && sT[keep] > sv_min) ++keep;
   if (keep == 0) keep = 1;
