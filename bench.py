@@ -50,6 +50,12 @@ BP_TOL, BP_MAXIT, SV_MIN = 1e-8, 50, 1e-8
 # after its minimum, so every step runs 50 sweeps and the messages are noise.
 SEED = 25
 CPU_SAMPLE_STEPS = 5  # Floquet steps of the CPU reference sample
+# Served stream: 512 requests, Poisson arrivals 2 ms apart on average, L in
+# {4,6,8,10,12}, chi in {8,16,32}, depth in 4..16, theta_h in [0.2,1.2],
+# 8-term random observable each.  The whole stream is ~35 GPU-minutes of BP
+# work, so the bench serves its first SERVED_N requests (a prefix of the same
+# seeded stream; --served-requests changes it).
+SERVED_SEED, SERVED_TOTAL, SERVED_N = 25, 512, 8
 
 
 def workload(seed=SEED):
@@ -88,6 +94,124 @@ def kicked_ising_qasm(steps, theta_j, theta_h):
             out.append(f"rx({theta_h!r}) q[{i}];")
         out.append("barrier q;")
     return "\n".join(out) + "\n"
+
+
+def random_observable(rng, n_qubits, n_terms=8):
+    """n_terms Pauli strings on 1-4 distinct random qubits, letters uniform in
+    {X,Y,Z}, coefficients N(0,1), as `.txt` lines (rightmost char = qubit 0).
+    The reference's ClassifyOps keeps 1-qubit and adjacent 2-qubit terms."""
+    lines = []
+    for _ in range(n_terms):
+        k = int(rng.integers(1, 5))
+        qs = rng.choice(n_qubits, size=k, replace=False)
+        letters = rng.choice(list("XYZ"), size=k)
+        chars = ["I"] * n_qubits
+        for q, c in zip(qs, letters):
+            chars[n_qubits - 1 - int(q)] = str(c)
+        lines.append(f"{float(rng.normal())!r} " + "".join(chars))
+    return "\n".join(lines) + "\n"
+
+
+def served_stream(n, seed=SERVED_SEED, total=SERVED_TOTAL):
+    """The first n requests of the seeded served stream (all `total` are drawn
+    so that every n gives a prefix of the same stream)."""
+    rng = np.random.default_rng(seed)
+    reqs, t = [], 0.0
+    for _ in range(total):
+        t += float(rng.exponential(2e-3))
+        L = int(rng.choice([4, 6, 8, 10, 12]))
+        chi = int(rng.choice([8, 16, 32]))
+        depth = int(rng.integers(4, 17))
+        th = float(rng.uniform(0.2, 1.2))
+        reqs.append({"t": t, "L": L, "chi": chi, "depth": depth, "theta_h": th,
+                     "pauli": random_observable(rng, L * L)})
+    return reqs[:n]
+
+
+def run_served(tb, reqs, precision):
+    """Continuous batching (tnbp_server_*): requests are submitted at their
+    arrival times (host clock) and the server steps while any is in flight.
+    Latency = result available - arrival (host wall clock)."""
+    srv = tb.Server(precision, 0, 64)
+    t0 = time.perf_counter()
+    ids, fin, nxt = {}, {}, 0
+    try:
+        while len(fin) < len(reqs):
+            now = time.perf_counter() - t0
+            while nxt < len(reqs) and reqs[nxt]["t"] <= now:
+                r = reqs[nxt]
+                terms = tb.load_sparse_pauli(r["pauli"], tb.bond_square_lattice(r["L"], r["L"]))
+                ids[nxt] = srv.submit_kicked_ising(r["L"], r["chi"], r["depth"], THETA_J, r["theta_h"], terms,
+                                                   BP_TOL, BP_MAXIT, SV_MIN)
+                nxt += 1
+            if len(ids) == len(fin):
+                time.sleep(max(0.0, reqs[nxt]["t"] - now))
+                continue
+            srv.step()
+            now = time.perf_counter() - t0
+            for i, rid in ids.items():
+                if i not in fin:
+                    try:
+                        v = srv.result(rid)
+                    except tb.TnbpError:
+                        v = complex("nan")  # the request failed; the others go on
+                    if v is not None:
+                        fin[i] = (now, v)
+    finally:
+        srv.close()
+    lat = [fin[i][0] - reqs[i]["t"] for i in range(len(reqs))]
+    span = max(f[0] for f in fin.values()) - reqs[0]["t"]
+    return [fin[i][1] for i in range(len(reqs))], lat, span
+
+
+def run_plain_fifo(tb, reqs, precision):
+    """The plain per-job path (State / AbsorbTPO / BeliefPropagationLoop /
+    Truncation / MeasurePauliSum), one request at a time in arrival order."""
+    t0 = time.perf_counter()
+    vals, lat, conv = [], [], []
+    for r in reqs:
+        now = time.perf_counter() - t0
+        if now < r["t"]:
+            time.sleep(r["t"] - now)
+        edges = tb.bond_square_lattice(r["L"], r["L"])
+        layer = tb.KickedIsingTPO(edges, THETA_J / 2, 0.0, r["theta_h"] / 2, 1.0)
+        ok = True
+        with tb.State(edges, precision) as st:
+            tpo = st.tpo(layer)
+            for _ in range(r["depth"]):
+                tb.AbsorbTPO(st, tpo)
+                _, c = tb.BeliefPropagationLoop(st, BP_TOL, BP_MAXIT)
+                ok = ok and c < BP_TOL
+                tb.Truncation(st, r["chi"], SV_MIN)
+            tot, _ = tb.MeasurePauliSum(st, tb.load_sparse_pauli(r["pauli"], edges))
+        vals.append(tot)
+        conv.append(ok)
+        lat.append(time.perf_counter() - t0 - r["t"])
+    span = time.perf_counter() - t0 - reqs[0]["t"]
+    return vals, lat, span, conv
+
+
+def served_summary(tb, n):
+    reqs = served_stream(n)
+    mixed, lat_m, span_m = run_served(tb, reqs, tb.MIXED)
+    plain, lat_p, span_p, conv = run_plain_fifo(tb, reqs, tb.C128)
+    dE = [abs(a - b) for a, b in zip(mixed, plain)]
+    dE_conv = [d for d, c in zip(dE, conv) if c]
+
+    def pct(x, q):
+        return float(np.percentile(np.asarray(x) * 1e3, q))
+    return {
+        "sample": f"first {n} of the seeded {SERVED_TOTAL}-request stream (seed {SERVED_SEED}): Poisson arrivals "
+                  "mean 2 ms, L in {4..12 even}, chi in {8,16,32}, depth 4-16, theta_h U[0.2,1.2], "
+                  "8-term random observable; latencies on the host clock",
+        "requests": [[r["L"], r["chi"], r["depth"], round(r["theta_h"], 4)] for r in reqs],
+        "mixed_served": {"solves_per_s": n / span_m, "p50_ms": pct(lat_m, 50), "p99_ms": pct(lat_m, 99)},
+        "plain_fp64_fifo": {"solves_per_s": n / span_p, "p50_ms": pct(lat_p, 50), "p99_ms": pct(lat_p, 99)},
+        "speedup": span_p / span_m,
+        "fp64_bp_converged": conv,
+        "dE_max_bp_converged": max(dE_conv) if dE_conv else None,
+        "dE_per_request": dE,
+    }
 
 
 class ClockSampler:
@@ -163,7 +287,7 @@ def solve(tb, precision, theta_h, pauli_text, resident=None, events=None):
         d2h += st.ne * 12
     total, per = tb.MeasurePauliSum(st, terms)
     d2h += 16 + 16 * len(per)
-    stats = dict(sweeps=sweeps, totals=st.sweep_totals(), h2d=h2d, d2h=d2h)
+    stats = dict(sweeps=sweeps, totals=st.sweep_totals(), h2d=h2d, d2h=d2h, per=per)
     st.close()
     return total, stats
 
@@ -190,7 +314,7 @@ def run_ours(args, rank, world, local_rank):
 
     # warm-up (untimed): same work as a timed step
     for _ in range(args.warmup):
-        solve(tb, tb.C64, theta_h, pauli_text)
+        solve(tb, tb.MIXED, theta_h, pauli_text)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -204,7 +328,7 @@ def run_ours(args, rank, world, local_rank):
             e0 = torch.cuda.Event(enable_timing=True)
             e0.record()
             ev_e2e0.append(e0)
-            s, stt = solve(tb, tb.C64, theta_h, pauli_text, events=ev_res)
+            s, stt = solve(tb, tb.MIXED, theta_h, pauli_text, events=ev_res)
             torch.cuda.synchronize()
             e1 = torch.cuda.Event(enable_timing=True)
             e1.record()
@@ -248,7 +372,7 @@ def run_ours(args, rank, world, local_rank):
         except (OSError, ValueError):
             traffic = None
     line = {
-        "metric": "estimator solves/s (mixed complex64 path; plain FP64 GPU path and |dE| beside)",
+        "metric": "estimator solves/s (mixed path; plain FP64 GPU path and |dE| beside)",
         "value": value,
         "unit": "solves/s",
         "n_gpus": world,
@@ -258,7 +382,8 @@ def run_ours(args, rank, world, local_rank):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "c64 (FP32 products, FP64 sums and FP64 truncation eigensolves)",
+        "dtype": "mixed: c64 BP sweeps (3xTF32 / FP32 products, FP64 sums) on a c128 state; FP64 absorb, "
+                 "truncation, measurement",
         "data": "synthetic (seeded kicked-Ising circuit and Pauli observable)",
         "config": {"workload": f"kicked-Ising {L_SIDE}x{L_SIDE} open PEPS, {STEPS} steps, chi={CHI}, "
                                "RZZ(-pi/4), RX(theta_h)",
@@ -302,7 +427,20 @@ def run_ours(args, rank, world, local_rank):
         line["plain_fp64"] = {"solves_per_s": 1e3 / ms64, "observable": [s64.real, s64.imag],
                               "bp_sweeps": st64["sweeps"], "sweep_ms": st64["totals"][0] / max(1, st64["totals"][3])}
         line["dE_vs_fp64"] = abs(sums[-1] - s64)
+        line["dterm_max_vs_fp64"] = float(np.max(np.abs(stats[-1]["per"] - st64["per"])))
+        # complex64 storage throughout (TNBP_C64): faster, but its rounding
+        # of the state each step limits the aggregated observable
+        torch.cuda.synchronize()
+        e0.record()
+        s32, st32 = solve(tb, tb.C64, theta_h, pauli_text)
+        e1.record()
+        torch.cuda.synchronize()
+        line["c64_storage"] = {"solves_per_s": 1e3 / e0.elapsed_time(e1), "bp_sweeps": st32["sweeps"],
+                               "dE_vs_fp64": abs(s32 - s64),
+                               "dterm_max_vs_fp64": float(np.max(np.abs(st32["per"] - st64["per"])))}
         line["speedup_vs_fp64"] = line["plain_fp64"]["solves_per_s"] and e2e_value / line["plain_fp64"]["solves_per_s"]
+    if args.served_requests > 0:
+        line["served"] = served_summary(tb, args.served_requests)
     if world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_sample(theta_h)
     print(json.dumps(line))
@@ -352,7 +490,7 @@ def run_reference(args, rank, world):
     value = float(np.mean(v)) if v else None
     line = {
         "impl": "reference",
-        "metric": "estimator solves/s (mixed complex64 path; plain FP64 GPU path and |dE| beside)",
+        "metric": "estimator solves/s (mixed path; plain FP64 GPU path and |dE| beside)",
         "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": (1e3 / value) if value else None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded kicked-Ising circuit and Pauli observable)",
@@ -374,6 +512,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--served-requests", type=int, default=SERVED_N,
+                    help="requests of the served stream to run (0 skips the served leg)")
     ap.add_argument("--lattice", type=int, default=L_SIDE,
                     help="lattice side (default 16; smaller sides are for profiling captures only)")
     ap.add_argument("--nsteps", type=int, default=STEPS,
