@@ -16,7 +16,7 @@ LIB = os.path.join(HERE, "libtnbp_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["engine.cu", "capi.cu", "server.cu", "noalloc.cu", "host_setup.cpp"]
+SOURCES = ["engine.cu", "capi.cu", "server.cu", "noalloc.cu", "host_setup.cpp", "trace.cpp"]
 
 
 def _headers():

@@ -24,6 +24,9 @@
 #include "kernels.cuh"
 #include "measure.cuh"
 #include "tc_leg.cuh"
+#include "tc_leg_bulk.cuh"
+#include "tc_gram.cuh"
+#include "trace.h"
 #include "truncate.cuh"
 
 namespace tnbp {
@@ -175,6 +178,7 @@ Job::~Job() {
   destroy_graphs();
   cudaStreamSynchronize(stream);
   V.release(); M[0].release(); M[1].release(); V32.release();
+  ws_scratch.release(); ws_chain[0].release(); ws_chain[1].release(); Vspare.release();
   plan = SweepPlan();
   if (host_scalar) cudaFreeHost(host_scalar);
   if (ev0) cudaEventDestroy(ev0);
@@ -239,7 +243,8 @@ void Job::get_complex(const DevBuf& src, double* dst, size_t n, size_t elem_off)
 }
 
 uint64_t Job::device_bytes() const {
-  return V.bytes + M[0].bytes + M[1].bytes + V32.bytes + plan.bytes();
+  return V.bytes + M[0].bytes + M[1].bytes + V32.bytes + ws_scratch.bytes + ws_chain[0].bytes +
+         ws_chain[1].bytes + Vspare.bytes + plan.bytes();
 }
 void Job::check_budget() const {
   if (budget && device_bytes() > budget)
@@ -253,14 +258,14 @@ void* Job::sweep_vptr(int s) const {
 }
 
 // TNBP_MIXED: round the complex128 site tensors to the complex64 copy that
-// the sweeps read.  A re-allocated copy invalidates the sweep plan (its
-// tasks and graphs hold the old addresses).
+// the sweeps read (the copy only grows).  A re-allocated copy invalidates the
+// sweep plan (its tasks and graphs hold the old addresses).
 void Job::sync_shadow() {
   if (prec != TNBP_MIXED || !shadow_dirty) return;
-  if (!V32.p || V32.bytes != v_elems * 8) {
+  TNBP_TRACE_SCOPE("sweep.sync_shadow");
+  if (V32.ensure(v_elems * 8, stream)) {
     destroy_graphs();
     plan = SweepPlan();
-    V32.alloc(v_elems * 8, stream);
   }
   const unsigned grid = (unsigned)std::min<size_t>((v_elems + 255) / 256, (size_t)8 * num_sms());
   k_narrow<<<grid, 256, 0, stream>>>(static_cast<const double2*>(V.p), static_cast<float2*>(V32.p), v_elems);
@@ -291,6 +296,9 @@ SweepBatch& SweepBatch::operator=(SweepBatch&& o) noexcept {
     sum_tasks = std::move(o.sum_tasks);
     cond = std::move(o.cond);
     gram_ntask = o.gram_ntask; nmsg = o.nmsg; nsum = o.nsum; gram_nblocks = o.gram_nblocks;
+    gtc_tasks = std::move(o.gtc_tasks);
+    gtc_begins = std::move(o.gtc_begins);
+    gtc_ntask = o.gtc_ntask; gtc_nblocks = o.gtc_nblocks;
     nkernels = o.nkernels;
     graph = o.graph;
     o.graph = nullptr;
@@ -298,14 +306,16 @@ SweepBatch& SweepBatch::operator=(SweepBatch&& o) noexcept {
   return *this;
 }
 uint64_t SweepBatch::bytes() const {
-  uint64_t b = gram_tasks.bytes + gram_begins.bytes + msg_tasks.bytes + sum_tasks.bytes + cond.bytes;
-  for (auto& l : levels) b += l.tasks.bytes + l.begins.bytes;
+  uint64_t b = gram_tasks.bytes + gram_begins.bytes + msg_tasks.bytes + sum_tasks.bytes + cond.bytes +
+               gtc_tasks.bytes + gtc_begins.bytes;
+  for (auto& l : levels)
+    b += l.tasks.bytes + l.begins.bytes + l.tc_tasks.bytes + l.tc_begins.bytes + l.bk_tasks.bytes + l.bk_begins.bytes;
   return b;
 }
 
 SweepPlan::~SweepPlan() {}
 uint64_t SweepPlan::bytes() const {
-  return scratch.bytes + partial.bytes + dist.bytes + single[0].bytes() + single[1].bytes();
+  return partial.bytes + dist.bytes + single[0].bytes() + single[1].bytes();
 }
 
 // --------------------------------------------------------------- sweep plan
@@ -360,6 +370,7 @@ struct SitePlanner {
 }  // namespace
 
 void Job::build_plan() {
+  TNBP_TRACE_SCOPE("sweep.build_plan");
   destroy_graphs();
   plan = SweepPlan();
   const int ns = (int)g.labels.size();
@@ -383,10 +394,10 @@ void Job::build_plan() {
   std::vector<size_t> slot_base(ns, 0);
   size_t o = 0;
   for (int s = 0; s < ns; ++s) { slot_base[s] = o; o += (size_t)nslots[s] * align_elems(site_elems(s)); }
-  plan.scratch.alloc(std::max<size_t>(o, 32) * wsz, stream);
+  ws_scratch.ensure(std::max<size_t>(o, 32) * wsz, stream);
   auto slot_ptr = [&](int s, int slot) -> void* {
     if (slot < 0) return sweep_vptr(s);
-    return static_cast<char*>(plan.scratch.p) + (slot_base[s] + (size_t)slot * align_elems(site_elems(s))) * wsz;
+    return static_cast<char*>(ws_scratch.p) + (slot_base[s] + (size_t)slot * align_elems(site_elems(s))) * wsz;
   };
   int maxlevel = 0;
   for (auto& op : ops) maxlevel = std::max(maxlevel, op.level + 1);
@@ -479,6 +490,7 @@ void Job::build_plan() {
 // parity) into one set of launches; block offsets are re-based so uneven
 // jobs share every launch.
 void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStream_t stream) {
+  TNBP_TRACE_SCOPE("sweep.build_batch");
   b.reset_graph();
   size_t nlev = 0;
   for (auto& e : entries) {
@@ -486,21 +498,28 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
     nlev = std::max(nlev, e.job->plan.levels.size());
   }
   b.levels.resize(nlev);
-  // The kernel is chosen per task, never per launch: complex64 tasks with
-  // Din, Dout <= 32 run on the tcgen05 kernel, every other task on the
-  // CUDA-core kernel, whatever else shares the batch.  A request's rounding
-  // therefore does not depend on what it is batched with.
+  // The kernel is chosen per task, never per launch: complex64 tasks whose
+  // tile is a contiguous byte range (tc::bulk_mode) run on the bulk-staged
+  // tcgen05 kernel, other tasks with Din, Dout <= 32 on the register-staged
+  // tcgen05 kernel, every other task on the CUDA-core kernel, whatever else
+  // shares the batch.  A request's rounding therefore does not depend on
+  // what it is batched with.
   const bool tc_ok = !entries.empty() && reduced_sweeps(entries[0].job->prec) && tcgen05_enabled();
   for (size_t lv = 0; lv < nlev; ++lv) {
-    std::vector<LegTask> t, t2;
-    std::vector<long long> beg, b2;
-    long long nb = 0, nb2 = 0;
+    std::vector<LegTask> t, t2, t3;
+    std::vector<long long> beg, b2, b3;
+    long long nb = 0, nb2 = 0, nb3 = 0;
     int maxdin = 1;
     for (auto& e : entries) {
       const auto& P = e.job->plan;
       if (lv >= P.levels.size()) continue;
       for (LegTask lt : P.levels[lv].tasks[e.parity]) {
-        if (tc_ok && lt.Din <= tc::kTcMaxD && lt.Dout <= tc::kTcMaxD) {
+        if (tc_ok && tc::bulk_mode(lt.L, lt.Din, lt.Dout) != 0) {
+          lt.block_begin = nb3;
+          b3.push_back(nb3);
+          nb3 += (lt.L * lt.R + tc::kTcRows - 1) / tc::kTcRows;
+          t3.push_back(lt);
+        } else if (tc_ok && lt.Din <= tc::kTcMaxD && lt.Dout <= tc::kTcMaxD) {
           lt.block_begin = nb2;
           b2.push_back(nb2);
           nb2 += (lt.L * lt.R + tc::kTcRows - 1) / tc::kTcRows;
@@ -525,16 +544,29 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
     L.tc_ntask = (int)t2.size();
     L.tc_nblocks = nb2;
     L.tc_smem = tc::leg_smem_bytes();
+    upload_vec(L.bk_tasks, t3, stream);
+    upload_vec(L.bk_begins, b3, stream);
+    L.bk_ntask = (int)t3.size();
+    L.bk_nblocks = nb3;
   }
-  std::vector<GramTask> gt;
-  std::vector<long long> gb;
+  // Gram tasks: per task, the tcgen05 kernel (one CTA per chunk) for the
+  // complex64 sweeps with C <= 32, else the CUDA-core kernel
+  std::vector<GramTask> gt, gt2;
+  std::vector<long long> gb, gb2;
   std::vector<MsgTask> mt;
   std::vector<SumTask> st;
-  long long nb = 0;
+  long long nb = 0, nb2 = 0;
   for (size_t ei = 0; ei < entries.size(); ++ei) {
     const auto& P = entries[ei].job->plan;
     for (size_t i = 0; i < P.gram.size(); ++i) {
       GramTask g1 = P.gram[i];
+      if (tc_ok && tc::gram_tc_ok(g1.C, g1.P)) {
+        g1.block_begin = nb2;
+        gb2.push_back(nb2);
+        nb2 += g1.nchunk;
+        gt2.push_back(g1);
+        continue;
+      }
       g1.block_begin = nb;
       gb.push_back(nb);
       nb += P.gram_blocks[i];
@@ -556,6 +588,10 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
   upload_vec(b.sum_tasks, st, stream);
   b.gram_ntask = (int)gt.size();
   b.gram_nblocks = nb;
+  upload_vec(b.gtc_tasks, gt2, stream);
+  upload_vec(b.gtc_begins, gb2, stream);
+  b.gtc_ntask = (int)gt2.size();
+  b.gtc_nblocks = nb2;
   b.nmsg = (int)mt.size();
   b.nsum = (int)st.size();
 }
@@ -579,6 +615,15 @@ template <typename R, typename MR>
 static int launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
   int n = 0;
   for (auto& lv : b.levels) {
+    if (lv.bk_ntask > 0) {
+      // persistent: one CTA per SM (about 193 KB of shared memory each)
+      const long long grid = std::min<long long>(lv.bk_nblocks, num_sms());
+      k_leg_apply_tc_bulk<MR><<<(unsigned)grid, 256, tc::bulk_smem_bytes(), stream>>>(
+          static_cast<const LegTask*>(lv.bk_tasks.p), static_cast<const long long*>(lv.bk_begins.p), lv.bk_ntask,
+          lv.bk_nblocks);
+      CK(cudaGetLastError());
+      ++n;
+    }
     if (lv.tc_ntask > 0) {
       // persistent: up to 2 CTAs per SM, each over a contiguous range of tiles
       const long long grid = std::min<long long>(lv.tc_nblocks, 2LL * num_sms());
@@ -596,13 +641,22 @@ static int launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
     CK(cudaGetLastError());
     ++n;
   }
+  if (b.gtc_ntask) {
+    k_gram_tc<<<(unsigned)b.gtc_nblocks, 256, tc::gram_smem_bytes(), stream>>>(
+        static_cast<const GramTask*>(b.gtc_tasks.p), static_cast<const long long*>(b.gtc_begins.p), b.gtc_ntask);
+    CK(cudaGetLastError());
+    ++n;
+  }
   if (b.gram_ntask) {
     k_gram<R><<<(unsigned)b.gram_nblocks, kThreads, 0, stream>>>(
         static_cast<const GramTask*>(b.gram_tasks.p), static_cast<const long long*>(b.gram_begins.p), b.gram_ntask);
     CK(cudaGetLastError());
+    ++n;
+  }
+  if (b.nmsg) {
     k_msg_finalize<R, MR><<<b.nmsg, kThreads, 0, stream>>>(static_cast<const MsgTask*>(b.msg_tasks.p));
     CK(cudaGetLastError());
-    n += 2;
+    ++n;
   }
   if (b.nsum) {
     k_segmented_sum<<<b.nsum, kThreads, 0, stream>>>(static_cast<const SumTask*>(b.sum_tasks.p));
@@ -626,6 +680,13 @@ static void tc_attr() {
   if (done) return;
   CK(cudaFuncSetAttribute(k_leg_apply_tc<MR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)tc::leg_smem_bytes()));
+  CK(cudaFuncSetAttribute(k_leg_apply_tc_bulk<MR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)tc::bulk_smem_bytes()));
+  static bool gram_done = false;
+  if (!gram_done) {
+    CK(cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::gram_smem_bytes()));
+    gram_done = true;
+  }
   done = true;
 }
 
@@ -680,6 +741,7 @@ void Job::run_sweep(int par) {
   if (!plan.valid) build_plan();
   SweepBatch& b = plan.single[par];
   if (!b.graph) {
+    TNBP_TRACE_SCOPE("sweep.graph_capture");
     prepare_kernels(prec);
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
@@ -702,6 +764,7 @@ void Job::run_sweep(int par) {
 }
 
 double Job::read_cond() {
+  TNBP_TRACE_SCOPE("sweep.cond_wait");
   CK(cudaMemcpyAsync(host_scalar, plan.single[last_par].cond.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
   if (reduced_sweeps(prec)) check_tc_error(stream);
@@ -749,6 +812,7 @@ bool stop_on_growth(int prec, double prev, double c) {
 }
 
 void Job::bp_run(double tol_in, int max_iter, int* iters, double* cond) {
+  TNBP_TRACE_SCOPE("bp_run");
   const double tol = effective_tol(prec, tol_in);
   *iters = 0;
   *cond = std::nan("");
@@ -775,6 +839,7 @@ void Job::bp_run(double tol_in, int max_iter, int* iters, double* cond) {
 Tpo::~Tpo() {}
 
 void Job::absorb_tpo(const Tpo& tpo) {
+  TNBP_TRACE_SCOPE("absorb");
   shadow_dirty = true;
   const int ns = (int)g.labels.size();
   const int ne = (int)g.edges.size();
@@ -786,8 +851,9 @@ void Job::absorb_tpo(const Tpo& tpo) {
   // new layout
   dim = ndim;
   layout();
-  DevBuf nV, nM0, nM1;
-  nV.alloc(v_elems * esz, stream);
+  DevBuf nM0, nM1;
+  DevBuf& nV = Vspare;
+  nV.ensure(v_elems * esz, stream);
   nM0.alloc(m_elems * esz, stream);
   nM1.alloc(m_elems * esz, stream);
   std::vector<AbsorbTask> at;
@@ -861,6 +927,7 @@ struct ChainEntry {
 };
 
 void Job::run_chains(std::vector<ChainEntry>& chains) {
+  TNBP_TRACE_SCOPE("chains");
   if (chains.empty()) return;
   size_t maxlen = 0;
   std::vector<size_t> base(chains.size());
@@ -877,9 +944,9 @@ void Job::run_chains(std::vector<ChainEntry>& chains) {
     tot += align_elems(mx);
     maxlen = std::max(maxlen, chains[i].legs.size());
   }
-  DevBuf buf[2];
-  buf[0].alloc(std::max<size_t>(tot, 32) * esz, stream);
-  buf[1].alloc(std::max<size_t>(tot, 32) * esz, stream);
+  DevBuf* buf = ws_chain;
+  buf[0].ensure(std::max<size_t>(tot, 32) * esz, stream);
+  buf[1].ensure(std::max<size_t>(tot, 32) * esz, stream);
   for (size_t lv = 0; lv < maxlen; ++lv) {
     std::vector<LegTask> t;
     std::vector<long long> b;
@@ -924,6 +991,7 @@ void Job::run_chains(std::vector<ChainEntry>& chains) {
 
 // --------------------------------------------------------------- truncation
 void Job::truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_out) {
+  TNBP_TRACE_SCOPE("truncate");
   shadow_dirty = true;
   if (chi_max < 1) throw Error(TNBP_EINVAL, "chi_max must be >= 1");
   const int ns = (int)g.labels.size();
@@ -970,17 +1038,20 @@ void Job::truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_ou
   CK(cudaGetLastError());
   std::vector<int> hkeep(ne), hstatus(ne);
   std::vector<double> herr(ne);
-  CK(cudaMemcpyAsync(hkeep.data(), keep.p, ne * sizeof(int), cudaMemcpyDeviceToHost, stream));
-  CK(cudaMemcpyAsync(herr.data(), err.p, ne * sizeof(double), cudaMemcpyDeviceToHost, stream));
-  CK(cudaMemcpyAsync(hstatus.data(), status.p, ne * sizeof(int), cudaMemcpyDeviceToHost, stream));
-  CK(cudaStreamSynchronize(stream));
+  {
+    TNBP_TRACE_SCOPE("truncate.svd_wait");
+    CK(cudaMemcpyAsync(hkeep.data(), keep.p, ne * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(herr.data(), err.p, ne * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(hstatus.data(), status.p, ne * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
   // new site tensors: V_s x_k P_k for every leg, then normalize
   const std::vector<int> odim = dim;
   const std::vector<size_t> ovoff = voff;
   dim.assign(hkeep.begin(), hkeep.end());
   layout();
-  DevBuf nV;
-  nV.alloc(v_elems * esz, stream);
+  DevBuf& nV = Vspare;
+  nV.ensure(v_elems * esz, stream);
   std::vector<ChainEntry> chains;
   {
     const std::vector<int> ndim = dim;
@@ -1004,7 +1075,6 @@ void Job::truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_ou
     voff = nvoff;
   }
   std::swap(V, nV);
-  nV.release();
   normalize_sites();
   // messages = diag(s)
   DevBuf nM0, nM1;
@@ -1044,6 +1114,7 @@ void Job::truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_ou
 }
 
 void Job::normalize_sites() {
+  TNBP_TRACE_SCOPE("normalize");
   shadow_dirty = true;
   const int ns = (int)g.labels.size();
   const int per_thread = 8;
@@ -1189,6 +1260,7 @@ void Job::compute_envs(const std::vector<int>& sites1, const std::vector<std::pa
 }
 
 void Job::measure_terms(const std::vector<TermSpec>& terms, double* values, double* sum) {
+  TNBP_TRACE_SCOPE("measure");
   // distinct one-site requests and two-site sides
   std::vector<int> sites1;
   std::map<int, int> pos1;

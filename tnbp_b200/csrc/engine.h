@@ -42,6 +42,13 @@ struct DevBuf {
     return *this;
   }
   ~DevBuf();
+  // Keep the buffer if it already holds nbytes; otherwise re-allocate
+  // (stream-ordered).  Returns true if the address changed.
+  bool ensure(size_t nbytes, cudaStream_t s) {
+    if (p && bytes >= nbytes) return false;
+    alloc(nbytes, s);
+    return true;
+  }
   void release();
   void alloc(size_t nbytes, cudaStream_t s);
 };
@@ -79,12 +86,20 @@ struct SweepBatch {
     DevBuf tc_tasks, tc_begins;
     int tc_ntask = 0;
     long long tc_nblocks = 0;
+    // tasks of the bulk-staged tcgen05 kernel (tc::bulk_mode != 0)
+    DevBuf bk_tasks, bk_begins;
+    int bk_ntask = 0;
+    long long bk_nblocks = 0;
     size_t tc_smem = 0;
   };
   std::vector<Level> levels;
   DevBuf gram_tasks, gram_begins, msg_tasks, sum_tasks, cond;
   int gram_ntask = 0, nmsg = 0, nsum = 0;
   long long gram_nblocks = 0;
+  // Gram tasks of the tcgen05 kernel (one CTA per chunk)
+  DevBuf gtc_tasks, gtc_begins;
+  int gtc_ntask = 0;
+  long long gtc_nblocks = 0;
   int nkernels = 0;
   cudaGraphExec_t graph = nullptr;
   SweepBatch() = default;
@@ -99,7 +114,7 @@ struct SweepBatch {
 
 struct SweepPlan {
   bool valid = false;
-  DevBuf scratch, partial, dist;
+  DevBuf partial, dist;
   std::vector<LevelHost> levels;
   std::vector<GramTask> gram;
   std::vector<long long> gram_blocks;  // blocks of each gram task
@@ -169,6 +184,12 @@ struct Job {
   // the first sweep after V changed
   DevBuf V32;
   bool shadow_dirty = true;
+  // Work buffers that only grow over the job's life, so that the Floquet
+  // steps do not return and re-map gigabytes through the allocator: the
+  // sweep's intermediate slots, the two chain buffers of truncation and
+  // measurement, and the spare site-tensor buffer that absorption and
+  // truncation write into before it is swapped with V.
+  DevBuf ws_scratch, ws_chain[2], Vspare;
   int cur = 0;
   int last_par = 0;
   SweepPlan plan;

@@ -133,8 +133,9 @@ template <typename R>
 __global__ void __launch_bounds__(kThreads) k_gram(const GramTask* __restrict__ tasks,
                                                    const long long* __restrict__ begins, int ntask) {
   using C = typename cvec<R>::type;
-  __shared__ C As[kRowTile][kColTile + 1];
-  __shared__ C Bs[kRowTile][kColTile + 1];
+  // rows padded to 34 elements: 16-byte aligned pairs for the 2x2 tiles
+  __shared__ __align__(16) C As[kRowTile][kColTile + 2];
+  __shared__ __align__(16) C Bs[kRowTile][kColTile + 2];
   const int ti = find_task(begins, ntask, blockIdx.x);
   const GramTask tk = tasks[ti];
   long long b = blockIdx.x - tk.block_begin;
@@ -153,6 +154,7 @@ __global__ void __launch_bounds__(kThreads) k_gram(const GramTask* __restrict__ 
   // accumulator, so rounding does not grow with the chunk length (up to 4096
   // rows); complex128 accumulates directly.
   constexpr bool kPromote = sizeof(R) == 4;
+  const int ga0 = 2 * (threadIdx.x % 16), gb0 = 2 * (threadIdx.x / 16);
   C acc[4];
   double2 accd[4];
 #pragma unroll
@@ -176,13 +178,20 @@ __global__ void __launch_bounds__(kThreads) k_gram(const GramTask* __restrict__ 
       Bs[qq][cc] = vb;
     }
     __syncthreads();
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int o = threadIdx.x + i * kThreads;
-      const int a = o % kColTile, bb = o / kColTile;
+    // each thread owns the 2x2 block (a0..a0+1, b0..b0+1) of the 32x32 tile:
+    // four smem reads per four complex FMAs
 #pragma unroll 8
-      for (int qq = 0; qq < kRowTile; ++qq) cfma_conj(acc[i], As[qq][a], Bs[qq][bb]);
-      if (kPromote) {
+    for (int qq = 0; qq < kRowTile; ++qq) {
+      const C x0 = As[qq][ga0], x1 = As[qq][ga0 + 1];
+      const C y0 = Bs[qq][gb0], y1 = Bs[qq][gb0 + 1];
+      cfma_conj(acc[0], x0, y0);
+      cfma_conj(acc[1], x1, y0);
+      cfma_conj(acc[2], x0, y1);
+      cfma_conj(acc[3], x1, y1);
+    }
+    if (kPromote) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
         const double2 t = to_d2(acc[i]);
         accd[i].x += t.x;
         accd[i].y += t.y;
@@ -193,8 +202,7 @@ __global__ void __launch_bounds__(kThreads) k_gram(const GramTask* __restrict__ 
   double2* part = tk.partial + (long long)chunk * tk.C * tk.C;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const int o = threadIdx.x + i * kThreads;
-    const int a = ca0 + o % kColTile, bb = cb0 + o / kColTile;
+    const int a = ca0 + ga0 + (i & 1), bb = cb0 + gb0 + (i >> 1);
     if (a < tk.C && bb < tk.C) part[a + (long long)tk.C * bb] = kPromote ? accd[i] : to_d2(acc[i]);
   }
 }

@@ -24,6 +24,7 @@
 #include "../../include/tnbp_b200.h"
 #include "host_setup.h"
 #include "server.h"
+#include "trace.h"
 
 namespace tnbp {
 
@@ -55,9 +56,9 @@ Server::~Server() {
 }
 
 // Peak device bytes of a kicked-Ising request on an L x L lattice: BP runs
-// at bond dimension 2*chi; per site the tensor, its copy during absorption
-// and truncation, the complex64 sweep copy (TNBP_MIXED) and the sweep
-// scratch slots of its degree; both message arenas twice; per-edge
+// at bond dimension 2*chi; per site the tensor, its spare buffer, the two
+// chain buffers of truncation, the complex64 sweep copy (TNBP_MIXED) and the
+// sweep scratch slots of its degree; both message arenas twice; per-edge
 // truncation work.
 uint64_t Server::footprint(const Request& r) const {
   const double esz = prec == TNBP_C64 ? 8.0 : 16.0;   // stored element
@@ -71,7 +72,7 @@ uint64_t Server::footprint(const Request& r) const {
       const int g = (x > 0) + (x < L - 1) + (y > 0) + (y < L - 1);
       const int slots = g == 4 ? 8 : g == 3 ? 5 : g == 2 ? 2 : 0;
       const double n = 2.0 * std::pow(D, g);
-      bytes += n * (2.0 * esz + shadow + wsz * slots);
+      bytes += n * (4.0 * esz + shadow + wsz * slots);  // V, spare, 2 chain buffers
     }
   const double ne = 2.0 * L * (L - 1);
   bytes += 4.0 * 2.0 * ne * D * D * esz;      // message arenas (old + new)
@@ -162,6 +163,7 @@ void Server::fail(Request& r, int code, const std::string& msg) {
 }
 
 void Server::step(int* n_active, int* n_queued, int* n_done) {
+  TNBP_TRACE_SCOPE("server.step");
   int done = 0;
   // 1. admission by HBM footprint and free slots
   while (!queue.empty() && (int)active.size() < max_active) {

@@ -108,6 +108,14 @@ __host__ __device__ constexpr size_t leg_smem_bytes() {
   return (size_t)2 * kTcRows * (2 * kTcMaxD) * 4 + (size_t)2 * (2 * kTcMaxD) * (2 * kTcMaxD) * 4 + 1024 + 64;
 }
 
+// One output row: out[l + L k] = (c[k], c[DQ + k]) for k < Dout.
+template <int DQ>
+__device__ __forceinline__ void store_row(float2* __restrict__ p, unsigned L, int Dout, const float* c) {
+#pragma unroll
+  for (int k = 0; k < DQ; ++k)
+    if (k < Dout) p[(size_t)L * k] = make_float2(c[k], c[DQ + k]);
+}
+
 }  // namespace tc
 
 // Persistent over a contiguous range of 128-row tiles: TMEM is allocated
@@ -154,17 +162,18 @@ __global__ void __launch_bounds__(128) k_leg_apply_tc(const LegTask* __restrict_
   int Din = 0, Dout = 0, Dp = 4, Dq = 8;
   float2 nxt[kTcMaxD];
   // issue the global loads of one tile row (thread = row) into registers
+  // Rows and row lengths of one task are < 2^31 (a site tensor has fewer
+  // than 2^31 elements), so the row split uses 32-bit division.
   auto load_row = [&](long long tile, int task_id) {
     const LegTask t = tasks[task_id];
-    const long long q = (tile - t.block_begin) * kTcRows + tid;
-    const long long rows = t.L * t.R;
-    const float2* __restrict__ in = static_cast<const float2*>(t.in);
+    const unsigned q = (unsigned)((tile - t.block_begin) * kTcRows) + (unsigned)tid;
+    const unsigned rows = (unsigned)(t.L * t.R), L = (unsigned)t.L;
     if (q < rows) {
-      const long long l = q % t.L, r = q / t.L;
-      const long long base = l + t.L * (long long)t.Din * r;
+      const unsigned l = q % L, r = q / L;
+      const float2* __restrict__ p =
+          static_cast<const float2*>(t.in) + (size_t)l + (size_t)L * (size_t)t.Din * r;
 #pragma unroll
-      for (int k = 0; k < kTcMaxD; ++k)
-        nxt[k] = k < t.Din ? __ldg(&in[base + t.L * k]) : make_float2(0.f, 0.f);
+      for (int k = 0; k < kTcMaxD; ++k) nxt[k] = k < t.Din ? __ldg(p + (size_t)L * k) : make_float2(0.f, 0.f);
     } else {
 #pragma unroll
       for (int k = 0; k < kTcMaxD; ++k) nxt[k] = make_float2(0.f, 0.f);
@@ -203,16 +212,34 @@ __global__ void __launch_bounds__(128) k_leg_apply_tc(const LegTask* __restrict_
       }
     }
     const int K2 = 2 * Dp, N2 = 2 * Dq;
-    // A operand for this tile from the prefetched registers
+    // A operand for this tile from the prefetched registers: per group of 4
+    // k one 16-byte store each of re-hi, im-hi, re-lo, im-lo.  A thread's
+    // row sits at a fixed offset inside every core matrix, and the imaginary
+    // half starts Dp/4 core-matrix columns further (Dp is a multiple of 4);
+    // a warp's 32 stores fill 512 contiguous bytes.
+    {
+      const uint32_t row_off = (uint32_t)((tid >> 3) * 128 + (tid & 7) * 16);
+      const uint32_t im_off = (uint32_t)(Dp >> 2) * (kTcRows * 16);
 #pragma unroll
-    for (int k = 0; k < kTcMaxD; ++k) {
-      if (k < Dp) {
-        const float re = nxt[k].x, im = nxt[k].y;
-        const float rh = to_tf32(re), ih = to_tf32(im);
-        *reinterpret_cast<float*>(a_hi + kmajor_off(tid, k, kTcRows)) = rh;
-        *reinterpret_cast<float*>(a_hi + kmajor_off(tid, Dp + k, kTcRows)) = ih;
-        *reinterpret_cast<float*>(a_lo + kmajor_off(tid, k, kTcRows)) = to_tf32(re - rh);
-        *reinterpret_cast<float*>(a_lo + kmajor_off(tid, Dp + k, kTcRows)) = to_tf32(im - ih);
+      for (int g4 = 0; g4 < kTcMaxD / 4; ++g4) {
+        if (4 * g4 < Dp) {
+          float4 rh, ih, rl, il;
+          float* prh = &rh.x; float* pih = &ih.x; float* prl = &rl.x; float* pil = &il.x;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const float re = nxt[4 * g4 + j].x, im = nxt[4 * g4 + j].y;
+            const float h1 = to_tf32(re), h2 = to_tf32(im);
+            prh[j] = h1;
+            pih[j] = h2;
+            prl[j] = to_tf32(re - h1);
+            pil[j] = to_tf32(im - h2);
+          }
+          const uint32_t o = (uint32_t)g4 * (kTcRows * 16) + row_off;
+          *reinterpret_cast<float4*>(a_hi + o) = rh;
+          *reinterpret_cast<float4*>(a_hi + o + im_off) = ih;
+          *reinterpret_cast<float4*>(a_lo + o) = rl;
+          *reinterpret_cast<float4*>(a_lo + o + im_off) = il;
+        }
       }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -255,17 +282,15 @@ __global__ void __launch_bounds__(128) k_leg_apply_tc(const LegTask* __restrict_
     const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
     tmem_ld32(lane_addr, c);
     if (N2 > 32) tmem_ld32(lane_addr + 32, c + 32);
-    const long long q = (tile - tk.block_begin) * kTcRows + tid;
-    if (q < tk.L * tk.R) {
-      const long long l = q % tk.L, r = q / tk.L;
-      float2* __restrict__ out = static_cast<float2*>(tk.out);
-      const long long obase = l + tk.L * (long long)Dout * r;
-#pragma unroll
-      for (int k = 0; k < kTcMaxD; ++k) {
-        if (k < Dout) {
-          const float im = (Dq == 8) ? c[8 + k] : (Dq == 16 ? c[16 + k] : (Dq == 24 ? c[24 + k] : c[32 + k]));
-          out[obase + tk.L * k] = make_float2(c[k], im);
-        }
+    const unsigned q = (unsigned)((tile - tk.block_begin) * kTcRows) + (unsigned)tid;
+    if (q < (unsigned)(tk.L * tk.R)) {
+      const unsigned L = (unsigned)tk.L, l = q % L, r = q / L;
+      float2* __restrict__ p = static_cast<float2*>(tk.out) + (size_t)l + (size_t)L * (size_t)Dout * r;
+      switch (Dq) {  // imaginary parts start at column Dq
+        case 8: store_row<8>(p, L, Dout, c); break;
+        case 16: store_row<16>(p, L, Dout, c); break;
+        case 24: store_row<24>(p, L, Dout, c); break;
+        default: store_row<32>(p, L, Dout, c); break;
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
