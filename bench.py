@@ -368,7 +368,7 @@ def run_ours(args, rank, world, local_rank):
     tp = os.path.join(ROOT, "profiles", "bp_sweep_traffic.json")
     if os.path.exists(tp):
         try:
-            traffic = json.load(open(tp)).get("dram_bytes_per_sweep_c64_16x16_chi16")
+            traffic = json.load(open(tp)).get("dram_bytes_per_sweep_mixed_16x16_chi16")
         except (OSError, ValueError):
             traffic = None
     line = {
