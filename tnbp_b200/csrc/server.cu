@@ -166,6 +166,7 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
   TNBP_TRACE_SCOPE("server.step");
   int done = 0;
   // 1. admission by HBM footprint and free slots
+  TNBP_TRACE_SCOPE("server.1_admit_absorb");
   while (!queue.empty() && (int)active.size() < max_active) {
     Request& r = *reqs[queue.front()];
     if (!active.empty() && in_use + r.footprint > budget) break;
@@ -196,6 +197,7 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
     }
   }
   if (!entries.empty()) {
+    TNBP_TRACE_SCOPE("server.3_sweep");
     for (auto* r : inbp) {
       r->job->sync_shadow();
       if (!r->job->plan.valid) r->job->build_plan();
@@ -234,6 +236,7 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
     }
   }
   // 4. truncation, next step or measurement
+  TNBP_TRACE_SCOPE("server.4_trunc_measure");
   for (int64_t id : active) {
     Request& r = *reqs[id];
     try {

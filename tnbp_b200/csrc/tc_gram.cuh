@@ -44,7 +44,9 @@ __host__ __device__ inline bool gram_tc_ok(int C, int P) { return P == 1 && C >=
 }  // namespace tc
 
 // grid: one CTA per chunk of every task; begins = exclusive prefix of nchunk
-__global__ void __launch_bounds__(256) k_gram_tc(const GramTask* __restrict__ tasks,
+// Two CTAs per SM (at most 128 registers per thread): while one CTA waits on
+// its loads or MMAs the other converts or drains.
+__global__ void __launch_bounds__(256, 2) k_gram_tc(const GramTask* __restrict__ tasks,
                                                  const long long* __restrict__ begins, int ntask) {
   using namespace tc;
   extern __shared__ __align__(1024) unsigned char tg_smem_raw[];
@@ -122,10 +124,14 @@ __global__ void __launch_bounds__(256) k_gram_tc(const GramTask* __restrict__ ta
   for (int i = 0; i < 32; ++i) acc[i] = 0.0;
   auto drain = [&](int buf) {
     if (32 * chalf < N2) {
-      float v[32];
-      tmem_ld32(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)buf * 64u + (uint32_t)(32 * chalf), v);
+      const uint32_t base = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)buf * 64u + (uint32_t)(32 * chalf);
 #pragma unroll
-      for (int i = 0; i < 32; ++i) acc[i] += (double)v[i];
+      for (int h = 0; h < 2; ++h) {
+        float v[16];
+        tmem_ld16(base + 16u * h, v);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) acc[16 * h + i] += (double)v[i];
+      }
     }
   };
 
