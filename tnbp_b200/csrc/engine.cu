@@ -514,7 +514,7 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
       const auto& P = e.job->plan;
       if (lv >= P.levels.size()) continue;
       for (LegTask lt : P.levels[lv].tasks[e.parity]) {
-        if (tc_ok && tc::bulk_mode(lt.L, lt.Din, lt.Dout) != 0) {
+        if (tc_ok && bulk_leg_enabled() && tc::bulk_mode(lt.L, lt.Din, lt.Dout) != 0) {
           lt.block_begin = nb3;
           b3.push_back(nb3);
           nb3 += (lt.L * lt.R + tc::kTcRows - 1) / tc::kTcRows;
@@ -719,6 +719,19 @@ bool tcgen05_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("TNBP_DISABLE_TCGEN05");
     return !(e && e[0] == '1');
+  }();
+  return on;
+}
+
+// The bulk-staged leg kernel (k_leg_apply_tc_bulk) is selected with
+// TNBP_LEG_BULK=1.  Default: the register-staged kernel, measured faster on
+// the 16x16 D = 32 sweep (30.9 ms vs 33.2 ms): with its 224 KB of shared
+// memory the bulk kernel runs one CTA per SM and is bound by the bytes it
+// keeps in flight, the register-staged one runs two.
+bool bulk_leg_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("TNBP_LEG_BULK");
+    return e && e[0] == '1';
   }();
   return on;
 }

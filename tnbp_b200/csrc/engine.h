@@ -141,6 +141,7 @@ bool stop_on_growth(int prec, double prev, double c);
 inline bool reduced_sweeps(int prec) { return prec != TNBP_C128; }
 void prepare_kernels(int prec);
 bool tcgen05_enabled();
+bool bulk_leg_enabled();
 int num_sms();
 void check_tc_error(cudaStream_t stream);
 
