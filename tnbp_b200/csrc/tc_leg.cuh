@@ -121,9 +121,18 @@ __host__ __device__ constexpr size_t leg_smem_bytes() {
   return (size_t)2 * kTcRows * (2 * kTcMaxD) * 4 + (size_t)2 * (2 * kTcMaxD) * (2 * kTcMaxD) * 4 + 1024 + 64;
 }
 
-// One output row: out[l + L k] = (c[k], c[DQ + k]) for k < Dout.
+// One output row: out[l + L k] = (c[k], c[DQ + k]) for k < Dout.  With
+// L == 1 and Dout even the row is contiguous and 16-byte aligned: two
+// complex numbers per store.
 template <int DQ>
 __device__ __forceinline__ void store_row(float2* __restrict__ p, unsigned L, int Dout, const float* c) {
+  if (L == 1 && (Dout & 1) == 0) {
+    float4* __restrict__ p4 = reinterpret_cast<float4*>(p);
+#pragma unroll
+    for (int k = 0; k < DQ; k += 2)
+      if (k < Dout) p4[k >> 1] = make_float4(c[k], c[DQ + k], c[k + 1], c[DQ + k + 1]);
+    return;
+  }
 #pragma unroll
   for (int k = 0; k < DQ; ++k)
     if (k < Dout) p[(size_t)L * k] = make_float2(c[k], c[DQ + k]);
@@ -181,7 +190,17 @@ __global__ void __launch_bounds__(128) k_leg_apply_tc(const LegTask* __restrict_
     const LegTask t = tasks[task_id];
     const unsigned q = (unsigned)((tile - t.block_begin) * kTcRows) + (unsigned)tid;
     const unsigned rows = (unsigned)(t.L * t.R), L = (unsigned)t.L;
-    if (q < rows) {
+    if (q < rows && L == 1 && (t.Din & 1) == 0) {
+      // contiguous, 16-byte aligned row (tensors are 256-byte aligned)
+      const float4* __restrict__ p4 = reinterpret_cast<const float4*>(static_cast<const float2*>(t.in) +
+                                                                      (size_t)t.Din * q);
+#pragma unroll
+      for (int k = 0; k < kTcMaxD; k += 2) {
+        const float4 v = k < t.Din ? __ldg(p4 + (k >> 1)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        nxt[k] = make_float2(v.x, v.y);
+        nxt[k + 1] = make_float2(v.z, v.w);
+      }
+    } else if (q < rows) {
       const unsigned l = q % L, r = q / L;
       const float2* __restrict__ p =
           static_cast<const float2*>(t.in) + (size_t)l + (size_t)L * (size_t)t.Din * r;
