@@ -102,6 +102,23 @@ __global__ void __launch_bounds__(256, 2) k_gram_tc(const GramTask* __restrict__
       const int item = tid + 256 * it;
       const int c = item & 31, q4 = item >> 5;
       unsigned q = q0 + 4u * q4, l = q % L, m = q / L;
+      if ((L & 3) == 0 && q + 3 < qe) {
+        // L % 4 == 0 and q multiple of 4: the four rows are 32 contiguous,
+        // 32-byte aligned bytes of column c
+        float4 a01 = make_float4(0.f, 0.f, 0.f, 0.f), a23 = a01, b01 = a01, b23 = a01;
+        if (c < C) {
+          const size_t off = (size_t)l + (size_t)L * c + (size_t)LC * m;
+          const float4* pa = reinterpret_cast<const float4*>(A + off);
+          const float4* pb = reinterpret_cast<const float4*>(B + off);
+          a01 = __ldg(pa); a23 = __ldg(pa + 1);
+          b01 = __ldg(pb); b23 = __ldg(pb + 1);
+        }
+        xa[it][0] = make_float2(a01.x, a01.y); xa[it][1] = make_float2(a01.z, a01.w);
+        xa[it][2] = make_float2(a23.x, a23.y); xa[it][3] = make_float2(a23.z, a23.w);
+        yb[it][0] = make_float2(b01.x, b01.y); yb[it][1] = make_float2(b01.z, b01.w);
+        yb[it][2] = make_float2(b23.x, b23.y); yb[it][3] = make_float2(b23.z, b23.w);
+        continue;
+      }
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         float2 va = make_float2(0.f, 0.f), vb = va;
