@@ -400,7 +400,7 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk.summary(),
     }
     line["roofline"] = {
-        "kernel": "BP sweep (k_leg_apply + k_gram + k_msg_finalize + k_segmented_sum, one CUDA graph)",
+        "kernel": "BP sweep (k_leg_apply_tc + k_gram_tc + k_msg_finalize + k_segmented_sum, one CUDA graph)",
         "bound": "tensor",
         "achieved": achieved,
         "peak": tf_peak,
