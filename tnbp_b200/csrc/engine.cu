@@ -26,6 +26,7 @@
 #include "tc_leg.cuh"
 #include "tc_leg_bulk.cuh"
 #include "tc_gram.cuh"
+#include "tc_leg64.cuh"
 #include "trace.h"
 #include "truncate.cuh"
 
@@ -299,6 +300,9 @@ SweepBatch& SweepBatch::operator=(SweepBatch&& o) noexcept {
     gtc_tasks = std::move(o.gtc_tasks);
     gtc_begins = std::move(o.gtc_begins);
     gtc_ntask = o.gtc_ntask; gtc_nblocks = o.gtc_nblocks;
+    g64_tasks = std::move(o.g64_tasks);
+    g64_begins = std::move(o.g64_begins);
+    g64_ntask = o.g64_ntask; g64_nblocks = o.g64_nblocks;
     nkernels = o.nkernels;
     graph = o.graph;
     o.graph = nullptr;
@@ -307,9 +311,10 @@ SweepBatch& SweepBatch::operator=(SweepBatch&& o) noexcept {
 }
 uint64_t SweepBatch::bytes() const {
   uint64_t b = gram_tasks.bytes + gram_begins.bytes + msg_tasks.bytes + sum_tasks.bytes + cond.bytes +
-               gtc_tasks.bytes + gtc_begins.bytes;
+               gtc_tasks.bytes + gtc_begins.bytes + g64_tasks.bytes + g64_begins.bytes;
   for (auto& l : levels)
-    b += l.tasks.bytes + l.begins.bytes + l.tc_tasks.bytes + l.tc_begins.bytes + l.bk_tasks.bytes + l.bk_begins.bytes;
+    b += l.tasks.bytes + l.begins.bytes + l.tc_tasks.bytes + l.tc_begins.bytes + l.bk_tasks.bytes +
+         l.bk_begins.bytes + l.t64_tasks.bytes + l.t64_begins.bytes;
   return b;
 }
 
@@ -506,9 +511,9 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
   // what it is batched with.
   const bool tc_ok = !entries.empty() && reduced_sweeps(entries[0].job->prec) && tcgen05_enabled();
   for (size_t lv = 0; lv < nlev; ++lv) {
-    std::vector<LegTask> t, t2, t3;
-    std::vector<long long> beg, b2, b3;
-    long long nb = 0, nb2 = 0, nb3 = 0;
+    std::vector<LegTask> t, t2, t3, t4;
+    std::vector<long long> beg, b2, b3, b4;
+    long long nb = 0, nb2 = 0, nb3 = 0, nb4 = 0;
     int maxdin = 1;
     for (auto& e : entries) {
       const auto& P = e.job->plan;
@@ -519,6 +524,11 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
           b3.push_back(nb3);
           nb3 += (lt.L * lt.R + tc::kTcRows - 1) / tc::kTcRows;
           t3.push_back(lt);
+        } else if (tc_ok && tc::leg64_ok(lt.Din, lt.Dout)) {
+          lt.block_begin = nb4;
+          b4.push_back(nb4);
+          nb4 += (lt.L * lt.R + tc::kTcRows - 1) / tc::kTcRows;
+          t4.push_back(lt);
         } else if (tc_ok && lt.Din <= tc::kTcMaxD && lt.Dout <= tc::kTcMaxD) {
           lt.block_begin = nb2;
           b2.push_back(nb2);
@@ -548,14 +558,18 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
     upload_vec(L.bk_begins, b3, stream);
     L.bk_ntask = (int)t3.size();
     L.bk_nblocks = nb3;
+    upload_vec(L.t64_tasks, t4, stream);
+    upload_vec(L.t64_begins, b4, stream);
+    L.t64_ntask = (int)t4.size();
+    L.t64_nblocks = nb4;
   }
   // Gram tasks: per task, the tcgen05 kernel (one CTA per chunk) for the
   // complex64 sweeps with C <= 32, else the CUDA-core kernel
-  std::vector<GramTask> gt, gt2;
-  std::vector<long long> gb, gb2;
+  std::vector<GramTask> gt, gt2, gt3;
+  std::vector<long long> gb, gb2, gb3;
   std::vector<MsgTask> mt;
   std::vector<SumTask> st;
-  long long nb = 0, nb2 = 0;
+  long long nb = 0, nb2 = 0, nb3 = 0;
   for (size_t ei = 0; ei < entries.size(); ++ei) {
     const auto& P = entries[ei].job->plan;
     for (size_t i = 0; i < P.gram.size(); ++i) {
@@ -565,6 +579,13 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
         gb2.push_back(nb2);
         nb2 += g1.nchunk;
         gt2.push_back(g1);
+        continue;
+      }
+      if (tc_ok && tc::gram64_ok(g1.C, g1.P)) {
+        g1.block_begin = nb3;
+        gb3.push_back(nb3);
+        nb3 += g1.nchunk;
+        gt3.push_back(g1);
         continue;
       }
       g1.block_begin = nb;
@@ -592,6 +613,10 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
   upload_vec(b.gtc_begins, gb2, stream);
   b.gtc_ntask = (int)gt2.size();
   b.gtc_nblocks = nb2;
+  upload_vec(b.g64_tasks, gt3, stream);
+  upload_vec(b.g64_begins, gb3, stream);
+  b.g64_ntask = (int)gt3.size();
+  b.g64_nblocks = nb3;
   b.nmsg = (int)mt.size();
   b.nsum = (int)st.size();
 }
@@ -624,6 +649,15 @@ static int launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
       CK(cudaGetLastError());
       ++n;
     }
+    if (lv.t64_ntask > 0) {
+      // persistent: one 256-thread CTA per SM (about 193 KB of shared memory)
+      const long long grid = std::min<long long>(lv.t64_nblocks, num_sms());
+      k_leg_apply_tc64<MR><<<(unsigned)grid, 256, tc::leg64_smem_bytes(), stream>>>(
+          static_cast<const LegTask*>(lv.t64_tasks.p), static_cast<const long long*>(lv.t64_begins.p),
+          lv.t64_ntask, lv.t64_nblocks);
+      CK(cudaGetLastError());
+      ++n;
+    }
     if (lv.tc_ntask > 0) {
       // persistent: up to 2 CTAs per SM, each over a contiguous range of tiles
       const long long grid = std::min<long long>(lv.tc_nblocks, 2LL * num_sms());
@@ -644,6 +678,12 @@ static int launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
   if (b.gtc_ntask) {
     k_gram_tc<<<(unsigned)b.gtc_nblocks, 256, tc::gram_smem_bytes(), stream>>>(
         static_cast<const GramTask*>(b.gtc_tasks.p), static_cast<const long long*>(b.gtc_begins.p), b.gtc_ntask);
+    CK(cudaGetLastError());
+    ++n;
+  }
+  if (b.g64_ntask) {
+    k_gram_tc64<<<(unsigned)b.g64_nblocks, 256, tc::gram64_smem_bytes(), stream>>>(
+        static_cast<const GramTask*>(b.g64_tasks.p), static_cast<const long long*>(b.g64_begins.p), b.g64_ntask);
     CK(cudaGetLastError());
     ++n;
   }
@@ -682,9 +722,13 @@ static void tc_attr() {
                           (int)tc::leg_smem_bytes()));
   CK(cudaFuncSetAttribute(k_leg_apply_tc_bulk<MR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)tc::bulk_smem_bytes()));
+  CK(cudaFuncSetAttribute(k_leg_apply_tc64<MR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)tc::leg64_smem_bytes()));
   static bool gram_done = false;
   if (!gram_done) {
     CK(cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::gram_smem_bytes()));
+    CK(cudaFuncSetAttribute(k_gram_tc64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)tc::gram64_smem_bytes()));
     gram_done = true;
   }
   done = true;

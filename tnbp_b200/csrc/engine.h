@@ -90,16 +90,20 @@ struct SweepBatch {
     DevBuf bk_tasks, bk_begins;
     int bk_ntask = 0;
     long long bk_nblocks = 0;
+    // tasks of the tcgen05 kernel for 32 < D <= 64
+    DevBuf t64_tasks, t64_begins;
+    int t64_ntask = 0;
+    long long t64_nblocks = 0;
     size_t tc_smem = 0;
   };
   std::vector<Level> levels;
   DevBuf gram_tasks, gram_begins, msg_tasks, sum_tasks, cond;
   int gram_ntask = 0, nmsg = 0, nsum = 0;
   long long gram_nblocks = 0;
-  // Gram tasks of the tcgen05 kernel (one CTA per chunk)
-  DevBuf gtc_tasks, gtc_begins;
-  int gtc_ntask = 0;
-  long long gtc_nblocks = 0;
+  // Gram tasks of the tcgen05 kernels (one CTA per chunk): C <= 32, 32 < C <= 64
+  DevBuf gtc_tasks, gtc_begins, g64_tasks, g64_begins;
+  int gtc_ntask = 0, g64_ntask = 0;
+  long long gtc_nblocks = 0, g64_nblocks = 0;
   int nkernels = 0;
   cudaGraphExec_t graph = nullptr;
   SweepBatch() = default;
