@@ -1,0 +1,54 @@
+"""tnbp_estimator (tnbp_b200/apps/estimator.cc): the estimator app's loop as
+C++ host code over the C ABI.
+
+Run with the reference app's command line on the golden circuits, its printed
+one- and two-site expectation values must equal the reference estimator's
+(the fixtures hold the values the reference printed) to 1e-9, as in
+test_gpu_parity.py's end-to-end test; --precision mixed must stay within
+1e-6 of them.
+"""
+import os
+import re
+import subprocess
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+from records import load_probe  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+APP = os.path.join(os.path.dirname(HERE), "tnbp_b200", "tnbp_estimator")
+ONE = re.compile(r"Expectation value of single site operator at site (\d+) (\S+)")
+TWO = re.compile(r"Expectation value of two site operator at sites \((\d+),(\d+)\) (\S+)")
+
+
+def _run(name, meta, precision):
+    if not os.path.exists(APP):
+        pytest.fail(f"{APP} is not built: run `python tnbp_b200/build.py`")
+    cmd = [APP, "--circuit", os.path.join(HERE, "golden", "inputs", f"{name}.qasm"),
+           "--sparse_pauli", os.path.join(HERE, "golden", "inputs", f"{name}.txt"),
+           "--max_bond_dim", str(meta["chi"]), "--bp_tolerance", repr(meta["tol"]),
+           "--max_bp_iterations", str(meta["maxit"]), "--sv_min", repr(meta["sv_min"]),
+           "--precision", precision, "--sum"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    one = [float(m.group(2)) for m in ONE.finditer(r.stdout)]
+    two = [float(m.group(3)) for m in TWO.finditer(r.stdout)]
+    return one, two, r.stdout
+
+
+@pytest.mark.parametrize("name", ["ki3x3", "rc3x3", "chain6"])
+@pytest.mark.parametrize("precision,tol", [("c128", 1e-9), ("mixed", 1e-6)])
+def test_estimator_app_prints_the_reference_values(name, precision, tol):
+    R, meta = load_probe(os.path.join(HERE, "golden", f"probe_{name}.npz"))
+    one, two, out = _run(name, meta, precision)
+    ref_one = [float(v.real) for v in R["meas1/values"]]
+    ref_two = [float(v.real) for v in R["meas2/values"]]
+    assert len(one) == len(ref_one), out
+    assert len(two) >= len(ref_two), out
+    for a, b in zip(one, ref_one):
+        assert abs(a - b) <= tol, (a, b)
+    for a, b in zip(two, ref_two):
+        assert abs(a - b) <= tol, (a, b)
+    assert "Sum of c_k <P_k>" in out

@@ -1,0 +1,179 @@
+// tnbp_estimator: the estimator app's loop (apps/estimator/main.cc:18-245)
+// as C++ host code over the C ABI of libtnbp_b200 (include/tnbp_b200.h), the
+// BP, truncation and measurement running on the B200.
+//
+// Command line as the reference app (apps/estimator/option.h:28-73):
+//   --circuit FILE  --sparse_pauli FILE  --max_bond_dim N  --bp_tolerance X
+//   --max_bp_iterations N  --sv_min X  --truncation_error X (accepted, unused
+//   by the reference too)  --backend default
+// plus --precision c128|mixed|c64 (default c128, the drop-in) and --sum
+// (print sum_k c_k <P_k>, which the reference does not compute).
+// Printed lines follow the reference's wording for the per-layer BP
+// condition, the per-edge truncation results and the per-term expectation
+// values (one-site terms first, then two-site terms, each in file order);
+// the reference's time stamps are left out.  Not supported here: the
+// ibm_kobe backend's fixed edge list, --num_gates manual layering and
+// --do_opt_tpo (OptTPObySVD), which are outside the BP hot path.
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "tnbp_b200.h"
+
+namespace {
+
+void check(int rc, const char* what) {
+  if (rc != TNBP_OK) throw std::runtime_error(std::string(what) + ": " + tnbp_last_error());
+}
+
+std::string read_file(const std::string& path) {
+  std::ifstream f(path);
+  if (!f) throw std::runtime_error("cannot open " + path);
+  std::stringstream ss;
+  ss << f.rdbuf();
+  return ss.str();
+}
+
+struct Options {
+  std::string backend = "default", circuit = "circuit.qasm", sparsepauli = "sparsepauliop.txt";
+  int max_bp_iterations = 50, max_bond_dim = 100;
+  double bp_tolerance = 1.0e-8, sv_min = 1.0e-8, truncation_error = 1.0e-8;
+  int precision = TNBP_C128;
+  bool print_sum = false;
+};
+
+Options parse(int argc, char** argv) {
+  Options o;
+  for (int i = 1; i < argc; ++i) {
+    const std::string a = argv[i];
+    auto next = [&]() -> std::string {
+      if (i + 1 >= argc) throw std::invalid_argument("missing value after " + a);
+      return argv[++i];
+    };
+    if (a == "--backend") o.backend = next();
+    else if (a == "--circuit") o.circuit = next();
+    else if (a == "--sparse_pauli") o.sparsepauli = next();
+    else if (a == "--max_bp_iterations") o.max_bp_iterations = std::atoi(next().c_str());
+    else if (a == "--bp_tolerance") o.bp_tolerance = std::atof(next().c_str());
+    else if (a == "--max_bond_dim") o.max_bond_dim = std::atoi(next().c_str());
+    else if (a == "--sv_min") o.sv_min = std::atof(next().c_str());
+    else if (a == "--truncation_error") o.truncation_error = std::atof(next().c_str());
+    else if (a == "--sum") o.print_sum = true;
+    else if (a == "--precision") {
+      const std::string p = next();
+      if (p == "c128") o.precision = TNBP_C128;
+      else if (p == "mixed") o.precision = TNBP_MIXED;
+      else if (p == "c64") o.precision = TNBP_C64;
+      else throw std::invalid_argument("--precision must be c128, mixed or c64");
+    } else if (a == "--num_gates" || a == "--do_opt_tpo" || a == "--eps_opt_tpo") {
+      throw std::invalid_argument(a + " is not supported by tnbp_estimator");
+    }
+  }
+  if (o.backend != "default") throw std::invalid_argument("only --backend default is supported");
+  return o;
+}
+
+int run(const Options& o) {
+  const std::string qasm = read_file(o.circuit);
+  // edges (EdgesFromQasm) and the greedy layering the reference prints
+  int64_t ne = 0;
+  check(tnbp_qasm_edges(qasm.c_str(), nullptr, 0, &ne), "tnbp_qasm_edges");
+  std::vector<int32_t> edges(2 * ne);
+  check(tnbp_qasm_edges(qasm.c_str(), edges.data(), ne, &ne), "tnbp_qasm_edges");
+  std::cout << " edges:";
+  for (int64_t e = 0; e < ne; ++e) std::cout << " (" << edges[2 * e] << "," << edges[2 * e + 1] << ")";
+  std::cout << "\n";
+
+  // one TPO layer per barrier block (QasmToTPO)
+  int32_t nlayers = 0;
+  int64_t nelems = 0;
+  check(tnbp_qasm_tpo(qasm.c_str(), edges.data(), ne, nullptr, nullptr, nullptr, 0, &nlayers, &nelems),
+        "tnbp_qasm_tpo");
+  int64_t ns = 0;
+  {
+    std::vector<char> seen;
+    for (int32_t v : edges) {
+      if ((size_t)v >= seen.size()) seen.resize(v + 1, 0);
+      seen[v] = 1;
+    }
+    for (char c : seen) ns += c;
+  }
+  std::vector<int32_t> rank((size_t)nlayers * ne);
+  std::vector<int64_t> off((size_t)nlayers * ns);
+  std::vector<double> data(2 * (size_t)nelems);
+  check(tnbp_qasm_tpo(qasm.c_str(), edges.data(), ne, rank.data(), off.data(), data.data(), nelems, &nlayers,
+                      &nelems),
+        "tnbp_qasm_tpo");
+
+  tnbp_job* job = nullptr;
+  check(tnbp_job_create(edges.data(), ne, nullptr, o.precision, nullptr, 0, &job), "tnbp_job_create");
+  std::vector<int32_t> dims(ne);
+  std::vector<double> errs(ne);
+  std::cout.precision(16);
+  for (int32_t t = 0; t < nlayers; ++t) {
+    // this layer's operators, re-based to its first element
+    int64_t base = off[(size_t)t * ns];
+    for (int64_t k = 0; k < ns; ++k) base = std::min(base, off[(size_t)t * ns + k]);
+    std::vector<int64_t> loff(ns);
+    for (int64_t k = 0; k < ns; ++k) loff[k] = off[(size_t)t * ns + k] - base;
+    tnbp_tpo* tpo = nullptr;
+    check(tnbp_tpo_create(job, rank.data() + (size_t)t * ne, loff.data(), data.data() + 2 * base, &tpo),
+          "tnbp_tpo_create");
+    check(tnbp_absorb_tpo(job, tpo), "tnbp_absorb_tpo");
+    check(tnbp_tpo_destroy(tpo), "tnbp_tpo_destroy");
+    int32_t iters = 0;
+    double cond = 0.0;
+    check(tnbp_bp_run(job, o.bp_tolerance, o.max_bp_iterations, &iters, &cond), "tnbp_bp_run");
+    std::cout << " error from belief propagation condition at step " << t << " = " << cond << " (" << iters
+              << " sweeps)\n";
+    check(tnbp_truncate(job, o.max_bond_dim, o.sv_min, dims.data(), errs.data()), "tnbp_truncate");
+    for (int64_t e = 0; e < ne; ++e)
+      std::cout << " truncation error for edge (" << edges[2 * e] << "," << edges[2 * e + 1] << ") = " << errs[e]
+                << " bond dim = " << dims[e] << "\n";
+  }
+
+  // measurement: load_sparse_pauli_op + SparsePauliToTensorOp + ClassifyOps
+  const std::string pauli = read_file(o.sparsepauli);
+  int64_t nk = 0, nd = 0;
+  check(tnbp_pauli_terms(pauli.c_str(), edges.data(), ne, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0,
+                         &nk, &nd),
+        "tnbp_pauli_terms");
+  std::vector<int32_t> kind(nk + 1), q0(nk + 1), q1(nk + 1), row(nk + 1);
+  std::vector<char> letters(2 * nk + 2);
+  std::vector<double> coeff(2 * nk + 2), per(2 * nk + 2), sum(2);
+  check(tnbp_pauli_terms(pauli.c_str(), edges.data(), ne, kind.data(), q0.data(), q1.data(), letters.data(),
+                         coeff.data(), row.data(), nk, &nk, &nd),
+        "tnbp_pauli_terms");
+  std::cout << " number of measrement operators = " << nk + nd << "\n";
+  if (nk > 0)
+    check(tnbp_measure_pauli_sum(job, nk, kind.data(), q0.data(), q1.data(), letters.data(), coeff.data(),
+                                 per.data(), sum.data()),
+          "tnbp_measure_pauli_sum");
+  for (int64_t k = 0; k < nk; ++k)
+    if (kind[k] == 1)
+      std::cout << " Expectation value of single site operator at site " << q0[k] << " " << per[2 * k] << "\n";
+  for (int64_t k = 0; k < nk; ++k)
+    if (kind[k] == 2)
+      std::cout << " Expectation value of two site operator at sites (" << q0[k] << "," << q1[k] << ") "
+                << per[2 * k] << "\n";
+  if (o.print_sum) std::cout << " Sum of c_k <P_k> = " << sum[0] << " " << sum[1] << "\n";
+  check(tnbp_job_destroy(job), "tnbp_job_destroy");
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  try {
+    return run(parse(argc, argv));
+  } catch (const std::exception& e) {
+    std::cerr << "tnbp_estimator: " << e.what() << "\n";
+    return 1;
+  }
+}

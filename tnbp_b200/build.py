@@ -13,6 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libtnbp_b200.so")
+APP = os.path.join(HERE, "tnbp_estimator")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -61,6 +62,15 @@ def build(verbose=True, jobs=4):
     if not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", LIB, "-lcudart_static",
                "-lrt", "-lpthread", "-ldl"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
+    # the estimator app over the C ABI (C++, host only)
+    app_src = os.path.join(HERE, "apps", "estimator.cc")
+    if os.path.exists(app_src) and (not os.path.exists(APP) or
+                                    max(os.path.getmtime(app_src), os.path.getmtime(LIB)) > os.path.getmtime(APP)):
+        cmd = ["g++", "-O2", "-std=c++17", "-I", INCLUDE, app_src, "-L", HERE, "-ltnbp_b200",
+               "-Wl,-rpath,$ORIGIN", "-o", APP]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
