@@ -142,9 +142,9 @@ __device__ __forceinline__ void store_row(float2* __restrict__ p, unsigned L, in
 
 // Persistent over a contiguous range of 128-row tiles: TMEM is allocated
 // once, the B operand is rebuilt only when the tile range crosses into a new
-// task, and the next tile's global loads are issued before waiting for the
-// current tile's MMAs so that loads, tensor-core work and the epilogue
-// overlap.
+// task, and the global loads of the tile after next are issued before
+// waiting for the current tile's MMAs so that loads, tensor-core work and
+// the epilogue overlap.
 template <typename MR>
 __global__ void __launch_bounds__(128) k_leg_apply_tc(const LegTask* __restrict__ tasks,
                                                       const long long* __restrict__ begins, int ntask,
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(128) k_leg_apply_tc(const LegTask* __restrict_
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(64u));
+                 "r"(128u));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
@@ -182,11 +182,13 @@ __global__ void __launch_bounds__(128) k_leg_apply_tc(const LegTask* __restrict_
   int cur_task = -1;
   LegTask tk;
   int Din = 0, Dout = 0, Dp = 4, Dq = 8;
-  float2 nxt[kTcMaxD];
+  // Two register buffers: tile i+2 is loaded into the buffer tile i was
+  // converted from, so a tile's loads have two tile periods to arrive.
+  float2 bufA[kTcMaxD], bufB[kTcMaxD];
   // issue the global loads of one tile row (thread = row) into registers
   // Rows and row lengths of one task are < 2^31 (a site tensor has fewer
   // than 2^31 elements), so the row split uses 32-bit division.
-  auto load_row = [&](long long tile, int task_id) {
+  auto load_row = [&](long long tile, int task_id, float2 (&nxt)[kTcMaxD]) {
     const LegTask t = tasks[task_id];
     const unsigned q = (unsigned)((tile - t.block_begin) * kTcRows) + (unsigned)tid;
     const unsigned rows = (unsigned)(t.L * t.R), L = (unsigned)t.L;
@@ -211,11 +213,46 @@ __global__ void __launch_bounds__(128) k_leg_apply_tc(const LegTask* __restrict_
       for (int k = 0; k < kTcMaxD; ++k) nxt[k] = make_float2(0.f, 0.f);
     }
   };
-  int task_of_next = find_task(begins, ntask, t_begin);
-  load_row(t_begin, task_of_next);
-  uint32_t phase = 0;
-  for (long long tile = t_begin; tile < t_end; ++tile) {
-    const int task_id = task_of_next;
+  // Double-buffered accumulator: the MMAs of tile i write TMEM columns
+  // [64 (i & 1), 64 (i & 1) + 64) while the threads drain tile i-1 from the
+  // other half.  One mbarrier: the k-th commit completes phase k & 1.
+  LegTask prev_tk{};
+  long long prev_q0 = 0;
+  int prev_Dq = 8;
+  int issued = -1;  // local index of the newest tile whose MMAs were committed
+  auto epilogue = [&](int li) {  // tile li's MMAs have completed
+    float c[64];
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(li & 1) * 64u;
+    tmem_ld32(lane_addr, c);
+    if (2 * prev_Dq > 32) tmem_ld32(lane_addr + 32, c + 32);
+    const unsigned q = (unsigned)prev_q0 + (unsigned)tid;
+    if (q < (unsigned)(prev_tk.L * prev_tk.R)) {
+      const unsigned L = (unsigned)prev_tk.L, l = q % L, r = q / L;
+      const int pDout = prev_tk.Dout;
+      float2* __restrict__ p = static_cast<float2*>(prev_tk.out) + (size_t)l + (size_t)L * (size_t)pDout * r;
+      switch (prev_Dq) {  // imaginary parts start at column Dq
+        case 8: store_row<8>(p, L, pDout, c); break;
+        case 16: store_row<16>(p, L, pDout, c); break;
+        case 24: store_row<24>(p, L, pDout, c); break;
+        default: store_row<32>(p, L, pDout, c); break;
+      }
+    }
+  };
+  // one tile: its task in slot (replaced by the task of tile + 2), its rows
+  // in nxt (replaced by the rows of tile + 2); false if a wait gave up
+  auto step = [&](long long tile, int& slot, float2 (&nxt)[kTcMaxD]) -> bool {
+    const int li = (int)(tile - t_begin);
+    const int task_id = slot;
+    // the MMAs of tile li - 1 read A and B: they must be done before both
+    // are rewritten
+    if (li > 0) {
+      const bool okw = mbar_wait(smem_u32(mbar), (uint32_t)((li - 1) & 1));
+      if (__syncthreads_or(!okw)) {
+        if (tid == 0) atomicExch(&g_tc_error, 1);
+        return false;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
     if (task_id != cur_task) {
       cur_task = task_id;
       tk = tasks[task_id];
@@ -279,60 +316,70 @@ __global__ void __launch_bounds__(128) k_leg_apply_tc(const LegTask* __restrict_
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (tid == 0) {
+      const uint32_t d = tmem + (uint32_t)(li & 1) * 64u;
       const uint32_t idesc = idesc_tf32(kTcRows, N2);
       const uint32_t a_lbo = kTcRows * 16, b_lbo = N2 * 16;
       const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo), bh = smem_u32(b_hi), bl = smem_u32(b_lo);
       for (int s = 0; s < K2 / 8; ++s) {
         const uint32_t ao = (uint32_t)s * 2 * a_lbo, bo = (uint32_t)s * 2 * b_lbo;
-        mma_tf32(tmem, smem_desc(ah + ao, a_lbo, 128), smem_desc(bh + bo, b_lbo, 128), idesc, s > 0 ? 1u : 0u);
-        mma_tf32(tmem, smem_desc(ah + ao, a_lbo, 128), smem_desc(bl + bo, b_lbo, 128), idesc, 1u);
-        mma_tf32(tmem, smem_desc(al + ao, a_lbo, 128), smem_desc(bh + bo, b_lbo, 128), idesc, 1u);
+        mma_tf32(d, smem_desc(ah + ao, a_lbo, 128), smem_desc(bh + bo, b_lbo, 128), idesc, s > 0 ? 1u : 0u);
+        mma_tf32(d, smem_desc(ah + ao, a_lbo, 128), smem_desc(bl + bo, b_lbo, 128), idesc, 1u);
+        mma_tf32(d, smem_desc(al + ao, a_lbo, 128), smem_desc(bh + bo, b_lbo, 128), idesc, 1u);
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                        smem_u32(mbar))
                    : "memory");
     }
-    // prefetch the next tile while the tensor cores work
-    if (tile + 1 < t_end) {
-      task_of_next = (tile + 1 >= tk.block_begin + ((tk.L * tk.R + kTcRows - 1) / kTcRows))
-                         ? find_task(begins, ntask, tile + 1)
-                         : task_id;
-      load_row(tile + 1, task_of_next);
+    issued = li;
+    // prefetch tile + 2 into the buffer just converted, while the tensor
+    // cores work
+    if (tile + 2 < t_end) {
+      slot = (tile + 2 >= tk.block_begin + ((tk.L * tk.R + kTcRows - 1) / kTcRows))
+                 ? find_task(begins, ntask, tile + 2)
+                 : task_id;
+      load_row(tile + 2, slot, nxt);
     }
-    const bool ok = mbar_wait(smem_u32(mbar), phase);
-    // the CTA leaves together if any thread gave up waiting; one more
-    // bounded wait lets MMAs still in flight drain before TMEM is freed
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) atomicExch(&g_tc_error, 1);
-      if (!ok) mbar_wait(smem_u32(mbar), phase);
-      break;
-    }
-    phase ^= 1u;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // epilogue: warp w holds tile rows 32w..32w+31 in TMEM lanes
-    float c[64];
-    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
-    tmem_ld32(lane_addr, c);
-    if (N2 > 32) tmem_ld32(lane_addr + 32, c + 32);
-    const unsigned q = (unsigned)((tile - tk.block_begin) * kTcRows) + (unsigned)tid;
-    if (q < (unsigned)(tk.L * tk.R)) {
-      const unsigned L = (unsigned)tk.L, l = q % L, r = q / L;
-      float2* __restrict__ p = static_cast<float2*>(tk.out) + (size_t)l + (size_t)L * (size_t)Dout * r;
-      switch (Dq) {  // imaginary parts start at column Dq
-        case 8: store_row<8>(p, L, Dout, c); break;
-        case 16: store_row<16>(p, L, Dout, c); break;
-        case 24: store_row<24>(p, L, Dout, c); break;
-        default: store_row<32>(p, L, Dout, c); break;
-      }
-    }
+    // epilogue of the previous tile from the other accumulator half
+    if (li > 0) epilogue(li - 1);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    prev_tk = tk;
+    prev_q0 = (tile - tk.block_begin) * kTcRows;
+    prev_Dq = Dq;
+    return true;
+  };
+  int slotA = find_task(begins, ntask, t_begin), slotB = 0;
+  load_row(t_begin, slotA, bufA);
+  if (t_begin + 1 < t_end) {
+    slotB = find_task(begins, ntask, t_begin + 1);
+    load_row(t_begin + 1, slotB, bufB);
+  }
+  bool ok_all = true;
+  long long tile = t_begin;
+  for (; tile < t_end; tile += 2) {
+    if (!step(tile, slotA, bufA)) { ok_all = false; break; }
+    if (tile + 1 < t_end && !step(tile + 1, slotB, bufB)) { ok_all = false; break; }
+  }
+  const int nt = (int)(t_end - t_begin);
+  if (ok_all) {  // the last tile
+    const bool okl = mbar_wait(smem_u32(mbar), (uint32_t)((nt - 1) & 1));
+    if (__syncthreads_or(!okl)) {
+      if (tid == 0) atomicExch(&g_tc_error, 1);
+      if (!okl) mbar_wait(smem_u32(mbar), (uint32_t)((nt - 1) & 1));
+    } else {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      epilogue(nt - 1);
+    }
+  } else {
+    // a wait gave up: give the newest committed MMAs one more bounded wait
+    // before TMEM is freed
+    if (tid == 0 && issued >= 0) mbar_wait(smem_u32(mbar), (uint32_t)(issued & 1));
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64u));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128u));
   }
 }
 
