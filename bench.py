@@ -292,6 +292,20 @@ def solve(tb, precision, theta_h, pauli_text, resident=None, events=None):
     return total, stats
 
 
+def max_over_ranks(dist, values, device):
+    """Element-wise maximum of per-rank timings (every rank gets it)."""
+    import torch
+    t = torch.tensor(values, device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def replica_value(world, steps, ms_max):
+    """Whole-job solves/s of `world` independent replicas that each ran
+    `steps` solves, timed by the slowest rank (weak scaling)."""
+    return world * steps / (ms_max / 1e3)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import tnbp_b200 as tb
@@ -344,15 +358,13 @@ def run_ours(args, rank, world, local_rank):
     e2e_ms = sum(a.elapsed_time(b) for a, b in zip(ev_e2e0, ev_end))
     res_ms = sum(a.elapsed_time(b) for a, b in zip(ev_res, ev_end))
     if dist:
-        t = torch.tensor([e2e_ms, res_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms, res_ms = float(t[0]), float(t[1])
+        e2e_ms, res_ms = max_over_ranks(dist, [e2e_ms, res_ms], "cuda")
     if rank != 0:
         dist.destroy_process_group()
         return
     K = args.steps
-    value = world * K / (res_ms / 1e3)
-    e2e_value = world * K / (e2e_ms / 1e3)
+    value = replica_value(world, K, res_ms)
+    e2e_value = replica_value(world, K, e2e_ms)
     tot_ms = sum(s["totals"][0] for s in stats)
     tot_fl = sum(s["totals"][1] for s in stats)
     tot_by = sum(s["totals"][2] for s in stats)
