@@ -112,6 +112,65 @@ def random_observable(rng, n_qubits, n_terms=8):
     return "\n".join(lines) + "\n"
 
 
+def random_circuit_workload(seed=SEED, L=10, layers=12):
+    """Random-circuit estimator: L x L qubits, `layers` layers of U3 (three
+    angles uniform in [0, 2pi)) on every qubit followed by CZ on one of four
+    edge colourings in cyclic order (horizontal even, horizontal odd,
+    vertical even, vertical odd), a barrier after each layer; 64-term random
+    observable.  Returns (qasm, pauli text)."""
+    rng = np.random.default_rng(seed)
+    n = L * L
+    out = ["OPENQASM 2.0;", 'include "qelib1.inc";', f"qreg q[{n}];"]
+    for layer in range(layers):
+        for i in range(n):
+            a, b, c = (float(x) for x in rng.uniform(0.0, 2 * math.pi, size=3))
+            out.append(f"u3({a!r},{b!r},{c!r}) q[{i}];")
+        col = layer % 4
+        for iy in range(L):
+            for ix in range(L):
+                i = ix + L * iy
+                if col < 2 and ix % 2 == col and ix + 1 < L:
+                    out.append(f"cz q[{i}],q[{i + 1}];")
+                if col >= 2 and iy % 2 == col - 2 and iy + 1 < L:
+                    out.append(f"cz q[{i}],q[{i + L}];")
+        out.append("barrier q;")
+    return "\n".join(out) + "\n", random_observable(rng, n, 64)
+
+
+def estimator_from_qasm(tb, precision, qasm, pauli, chi):
+    """QasmToTPO layers, then the estimator loop; returns (sum, terms kept,
+    terms dropped)."""
+    edges = tb.EdgesFromQasm(qasm)
+    layers = tb.QasmToTPO(qasm, edges)
+    terms = tb.load_sparse_pauli(pauli, edges)
+    with tb.State(edges, precision) as st:
+        for layer in layers:
+            tb.AbsorbTPO(st, layer)
+            tb.BeliefPropagationLoop(st, BP_TOL, BP_MAXIT)
+            tb.Truncation(st, chi, SV_MIN)
+        total, _ = tb.MeasurePauliSum(st, terms)
+    return total, len(terms), terms.dropped
+
+
+def random_circuit_summary(tb):
+    import torch
+    qasm, pauli = random_circuit_workload()
+    res = {}
+    for name, prec in (("mixed", tb.MIXED), ("plain_fp64", tb.C128)):
+        estimator_from_qasm(tb, prec, qasm, pauli, 32)  # warm-up
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        total, kept, dropped = estimator_from_qasm(tb, prec, qasm, pauli, 32)
+        torch.cuda.synchronize()
+        res[name] = {"solves_per_s": 1.0 / (time.perf_counter() - t), "sum": [total.real, total.imag]}
+    res["speedup"] = res["mixed"]["solves_per_s"] / res["plain_fp64"]["solves_per_s"]
+    res["dE"] = abs(complex(*res["mixed"]["sum"]) - complex(*res["plain_fp64"]["sum"]))
+    res["terms_kept"], res["terms_dropped"] = kept, dropped
+    res["workload"] = ("random circuit 10x10, 12 layers U3 + CZ (4 colourings, cyclic), chi 32, "
+                       "64-term observable (the reference drops >2-qubit and non-adjacent terms); host wall clock")
+    return res
+
+
 def served_stream(n, seed=SERVED_SEED, total=SERVED_TOTAL):
     """The first n requests of the seeded served stream (all `total` are drawn
     so that every n gives a prefix of the same stream)."""
@@ -453,6 +512,8 @@ def run_ours(args, rank, world, local_rank):
         line["speedup_vs_fp64"] = line["plain_fp64"]["solves_per_s"] and e2e_value / line["plain_fp64"]["solves_per_s"]
     if args.served_requests > 0:
         line["served"] = served_summary(tb, args.served_requests)
+    if not args.no_fp64:
+        line["random_circuit"] = random_circuit_summary(tb)
     if world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_sample(theta_h)
     print(json.dumps(line))
