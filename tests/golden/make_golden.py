@@ -256,6 +256,15 @@ def main():
         with open(os.path.join(INPUTS, "v3.qasm"), "w") as f:
             f.write(v3)
         run_hostparity("v3", ["qasm", os.path.join(INPUTS, "v3.qasm")])
+    if "host_rc10" in jobs:
+        # the benchmark's random-circuit workload (bench.py): 10x10, 12 layers
+        sys.path.insert(0, ROOT)
+        import bench
+        q, p = bench.random_circuit_workload()
+        for ext, txt in (("qasm", q), ("txt", p)):
+            with open(os.path.join(INPUTS, f"rc10x10.{ext}"), "w") as f:
+                f.write(txt)
+        run_hostparity("rc10x10", ["qasm", os.path.join(INPUTS, "rc10x10.qasm"), os.path.join(INPUTS, "rc10x10.txt")])
     if "config1" in jobs:
         run_config1()
 
