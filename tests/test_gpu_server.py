@@ -29,9 +29,11 @@ TOL_MIXED = 1e-6  # mixed server (complex128 state) vs the complex128 path
 # per-term errors reach ~1e-6 here, so that mode is held to 1e-5
 TOL_C64 = 1e-5
 
-# (L, chi, steps, theta_h, seed of the observable)
+# (L, chi, steps, theta_h, seed of the observable); the chi = 32 request
+# reaches BP at D = 64 in its last step, so the batches mix the D <= 32 and
+# the 32 < D <= 64 tensor-core kernels with the CUDA-core ones
 REQUESTS = [(4, 4, 4, 0.55, 1), (3, 8, 5, 0.30, 2), (5, 2, 3, 0.90, 3), (4, 8, 3, 1.10, 4),
-            (6, 4, 3, 0.70, 5), (3, 2, 6, 0.40, 6)]
+            (6, 4, 3, 0.70, 5), (3, 2, 6, 0.40, 6), (3, 32, 6, 0.45, 7)]
 
 
 def observable(L, seed, n_terms=8):
