@@ -127,6 +127,21 @@ int tnbp_kicked_ising_tpo(const int32_t* edges, int64_t n_edges, double Jz, doub
                           double hx, double dt, int32_t* edge_rank, int64_t* op_offset,
                           double* op_data, int64_t cap_elems, int64_t* n_elems_out);
 
+/* OptTPObySVD (include/tnbp/ptns/function/optsvdtpo.h:86-214) on one TPO
+   layer, in place, as the reference mutates its std::vector<TenT>: for every
+   edge in edge order the two site operators are contracted over their bond
+   and split again by a truncated SVD that keeps the singular values > eps
+   (at most the old bond dimension, at least one), sqrt(s) given to both
+   sides.  On entry edge_rank[n_edges], op_offset[n_sites] (complex-element
+   offsets relative to op_data) and op_data hold one layer in the layout of
+   tnbp_qasm_tpo; on return they hold the compressed layer packed from
+   op_data[0] in site order, n_elems_out its element count.  Bond dimensions
+   never grow, so a layer packed without overlaps always fits.  Host code
+   only (no device is used).  The reference app applies it to every layer
+   after QasmToTPO when run with --do_opt_tpo (apps/estimator/main.cc:88-94). */
+int tnbp_opt_tpo_svd(const int32_t* edges, int64_t n_edges, double eps, int32_t* edge_rank,
+                     int64_t* op_offset, double* op_data, int64_t* n_elems_out);
+
 /* ============================ device state =============================== */
 
 /* InitTensorProductState (include/tnbp/ptns/function/init.h:18-95): product

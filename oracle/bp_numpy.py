@@ -100,6 +100,41 @@ def absorb_tpo(edges, V, E, O):
     return nV, nE
 
 
+def opt_tpo_svd(edges, O, eps):
+    """OptTPObySVD (include/tnbp/ptns/function/optsvdtpo.h:86-214), step by
+    step: for each edge m = (a, b) in edge order, C = O_a contracted with
+    O_b over the bond (remaining legs of O_a, then of O_b, 162-164), an SVD
+    of C with O_a's legs as rows (173-174; kept: s > eps, at most the bond
+    dimension, at least one -- the TruncSVD rule), sqrt(s) to both sides
+    (175-181), O_a = U sqrt(s) with the new bond at its old leg position
+    (182-197), O_b = sqrt(s) V with the same (198-212).  O is a list of site
+    operators (r_0, ..., r_{g-1}, d_in, d_out); a new list is returned."""
+    sites = sites_of(edges)
+    pos = {s: i for i, s in enumerate(sites)}
+    O = [np.array(o, dtype=np.complex128) for o in O]
+    for m, (a, b) in enumerate(edges):
+        ia, ib = pos[a], pos[b]
+        pa = bonds_of(edges, a).index(m)
+        pb = bonds_of(edges, b).index(m)
+        A, B = O[ia], O[ib]
+        r = A.shape[pa]
+        C = np.tensordot(A, B, axes=([pa], [pb]))
+        rows = [A.shape[k] for k in range(A.ndim) if k != pa]
+        cols = [B.shape[k] for k in range(B.ndim) if k != pb]
+        M = C.reshape(int(np.prod(rows)), int(np.prod(cols)), order="F")
+        U, s, Vh = np.linalg.svd(M, full_matrices=False)
+        keep = 0
+        while keep < len(s) and keep < r and s[keep] > eps:
+            keep += 1
+        keep = max(keep, 1)
+        sq = np.sqrt(s[:keep])
+        Ua = (U[:, :keep] * sq[None, :]).reshape(rows + [keep], order="F")
+        Vb = (sq[:, None] * Vh[:keep, :]).reshape([keep] + cols, order="F")
+        O[ia] = np.moveaxis(Ua, -1, pa)
+        O[ib] = np.moveaxis(Vb, 0, pb)
+    return O
+
+
 # ------------------------------------------------------------------- BP
 def _absorb_leg(t, leg, M):
     """T_new[..., k', ...] = sum_j T[..., j, ...] M[j, k'] (bp.h:137-152)."""

@@ -7,7 +7,12 @@
 //
 // usage: ref_hostparity lattice <Lx> <Ly>
 //        ref_hostparity qasm <file.qasm> [<pauli.txt> [<Lx> <Ly>]]
+//        ref_hostparity opttpo <file.qasm> <eps> [<Lx> <Ly>]
+// (opttpo: every TPO layer of QasmToTPO before and after the reference's
+//  OptTPObySVD, include/tnbp/ptns/function/optsvdtpo.h, as shapes and
+//  column-major element lists)
 // (with Lx Ly the TPO and Pauli classification use bond_square_lattice)
+#include <chrono>
 #include <cstdio>
 #include <iostream>
 #include <sstream>
@@ -59,6 +64,24 @@ static void graph_json(const std::vector<std::pair<int, int>>& edges) {
   std::printf("]");
 }
 
+static void tpo_json(const char* key, const std::vector<std::vector<Tensor>>& T) {
+  std::printf("\"%s\": [", key);
+  for (size_t l = 0; l < T.size(); ++l) {
+    std::printf("%s[", l ? "," : "");
+    for (size_t s = 0; s < T[l].size(); ++s) {
+      auto sh = T[l][s].Shape();
+      std::printf("%s[[", s ? "," : "");
+      for (size_t k = 0; k < sh.size(); ++k) std::printf("%s%d", k ? "," : "", sh[k]);
+      std::printf("],[");
+      for (size_t k = 0; k < T[l][s].Size(); ++k)
+        std::printf("%s%.17g,%.17g", k ? "," : "", T[l][s].GetElem(k).real(), T[l][s].GetElem(k).imag());
+      std::printf("]]");
+    }
+    std::printf("]");
+  }
+  std::printf("]");
+}
+
 int main(int argc, char** argv) {
   if (argc < 3) { std::fprintf(stderr, "usage\n"); return 2; }
   const std::string mode = argv[1];
@@ -66,6 +89,22 @@ int main(int argc, char** argv) {
   if (mode == "lattice") {
     auto edges = tnbp::bond_square_lattice(std::atoi(argv[2]), std::atoi(argv[3]));
     graph_json(edges);
+  } else if (mode == "opttpo") {
+    auto prog = qasm::parse_any(qasm::read_all_file(argv[2]));
+    const double eps = std::atof(argv[3]);
+    auto edges = argc > 5 ? tnbp::bond_square_lattice(std::atoi(argv[4]), std::atoi(argv[5]))
+                          : tnbp::EdgesFromQasm(prog);
+    edges_json("edges", edges);
+    tci::gqten_handle ctx;
+    auto T = tnbp::QasmToTPO<Tensor>(ctx, prog, edges);
+    std::printf(", ");
+    tpo_json("before", T);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (auto& layer : T) tnbp::OptTPObySVD(ctx, edges, layer, eps);
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::printf(", ");
+    tpo_json("after", T);
+    std::printf(", \"eps\": %.17g, \"opt_seconds\": %.6g", eps, secs);
   } else if (mode == "qasm") {
     auto prog = qasm::parse_any(qasm::read_all_file(argv[2]));
     std::printf("\"instructions\": [");

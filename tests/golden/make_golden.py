@@ -13,6 +13,12 @@ oracle/_ref/, and this script runs them on seeded synthetic inputs:
   host_<name>.json   lattice edges, greedy layers, leg order, BFS paths,
                      parsed QASM instructions, TPO layer shapes, Pauli
                      classification (oracle/ref_hostparity.cc)
+  opttpo_<name>.npz  TPO layers before and after the reference's OptTPObySVD
+                     (small circuits: every site operator)
+  opttpo_kobe.json   the same on the reference's kicked_ising.qasm, reduced
+                     to gauge-invariant data (bond dimensions, per-leg
+                     singular values of every site operator)
+  opt_<name>.json    the estimator app's printed values with --do_opt_tpo 1
   config1.json       observables of the 4x4 kicked-Ising workload from the
                      reference apps kicked_ising_lattice and estimator
 
@@ -96,6 +102,98 @@ def random_circuit_qasm(Lx, Ly, layers, rng):
             out.append(f"cz q[{i}],q[{j}];")
         out.append("barrier q;")
     return "\n".join(out) + "\n"
+
+
+def zz_cx_qasm(Lx, Ly, steps, theta, theta_h):
+    """Kicked Ising with each ZZ rotation compiled as cx, rz, cx (the form of
+    the reference's apps/estimator/kicked_ising.qasm): operator rank 4 per
+    bond before OptTPObySVD, 2 after."""
+    n = Lx * Ly
+    out = ["OPENQASM 2.0;", 'include "qelib1.inc";', f"qreg q[{n}];"]
+    for _ in range(steps):
+        for (i, j) in lattice_edges_rect(Lx, Ly):
+            out += [f"cx q[{i}],q[{j}];", f"rz({theta!r}) q[{j}];", f"cx q[{i}],q[{j}];"]
+        for i in range(n):
+            out.append(f"rx({theta_h!r}) q[{i}];")
+        out.append("barrier q;")
+    return "\n".join(out) + "\n"
+
+
+def opt_mix_qasm():
+    """2x3 lattice: CZ twice on one edge (rank 4, compresses to 1), a
+    distance-2 cx (pass-through bonds), rzz and cx on one edge, U3s."""
+    lines = ["OPENQASM 2.0;", 'include "qelib1.inc";', "qreg q[6];"]
+    for (i, j) in lattice_edges_rect(3, 2):
+        lines.append(f"cz q[{i}],q[{j}];")
+    lines += ["cz q[0],q[1];", "u3(0.3,1.1,-0.4) q[1];", "cx q[0],q[2];", "rzz(0.37) q[4],q[5];",
+              "cx q[4],q[5];", "barrier q;", "h q[3];", "cz q[3],q[4];", "cz q[3],q[4];", "cx q[1],q[4];",
+              "barrier q;"]
+    return "\n".join(lines) + "\n"
+
+
+def leg_spectra(t):
+    """Singular values of every bond-leg unfolding of a site operator: equal
+    for two TPOs that differ by unitaries on their bonds."""
+    out = []
+    for k in range(t.ndim - 2):
+        out.append(np.linalg.svd(np.moveaxis(t, k, 0).reshape(t.shape[k], -1), compute_uv=False).tolist())
+    return out
+
+
+def run_opttpo(name, qasm_path, eps_list, lattice=None, full=True):
+    arrays = {}
+    summary = {}
+    for eps in eps_list:
+        args = [os.path.join(REF_BIN, "ref_hostparity"), "opttpo", qasm_path, repr(eps)]
+        if lattice:
+            args += [str(lattice[0]), str(lattice[1])]
+        d = json.loads(subprocess.check_output(args, text=True))
+        arrays["edges"] = np.array(d["edges"], np.int32)
+        tag = f"eps{eps:g}"
+        layers = []
+        for stage in ("before", "after"):
+            for l, layer in enumerate(d[stage]):
+                for s, (shape, flat) in enumerate(layer):
+                    a = np.array(flat, np.float64).reshape(-1, 2)
+                    t = (a[:, 0] + 1j * a[:, 1]).reshape(shape, order="F")
+                    if full:
+                        arrays[f"{tag}/{stage}/{l}/{s}"] = t
+                    elif stage == "after":
+                        while len(layers) <= l:
+                            layers.append([])
+                        layers[l].append(dict(shape=list(shape), norm=float(np.linalg.norm(t)),
+                                              legs=leg_spectra(t)))
+        summary[tag] = dict(eps=eps, layers=layers)
+    if full:
+        np.savez_compressed(os.path.join(HERE, f"opttpo_{name}.npz"), **arrays)
+    else:
+        summary["edges"] = arrays["edges"].tolist()
+        with open(os.path.join(HERE, f"opttpo_{name}.json"), "w") as f:
+            json.dump(summary, f, separators=(",", ":"))
+    print(f"opttpo_{name}: eps {eps_list}")
+
+
+def run_opt_estimator(name, qasm, pauli, chi, sv_min, tol, maxit, eps):
+    """The reference estimator app with --do_opt_tpo 1: its printed values."""
+    qp = os.path.join(INPUTS, f"{name}.qasm")
+    pp = os.path.join(INPUTS, f"{name}.txt")
+    with open(qp, "w") as f:
+        f.write(qasm)
+    with open(pp, "w") as f:
+        f.write(pauli)
+    out = subprocess.check_output(
+        [os.path.join(REF_BIN, "estimator"), "--circuit", qp, "--sparse_pauli", pp, "--max_bond_dim", str(chi),
+         "--bp_tolerance", repr(tol), "--max_bp_iterations", str(maxit), "--sv_min", repr(sv_min),
+         "--do_opt_tpo", "1", "--eps_opt_tpo", repr(eps)], text=True)
+    one = [float(v) for v in re.findall(r"single site operator at site \d+ (\S+)", out)]
+    two = [float(v) for v in re.findall(r"two site operator at sites \(\d+,\d+\) (\S+)", out)]
+    dims = [int(v) for v in re.findall(r"bond dim = (\d+)", out)]
+    conds = [float(v) for v in re.findall(r"condition at step \d+ = (\S+)", out)]
+    res = dict(chi=chi, sv_min=sv_min, tol=tol, maxit=maxit, eps_opt_tpo=eps, one=one, two=two, bond_dims=dims,
+               conditions=conds)
+    with open(os.path.join(HERE, f"opt_{name}.json"), "w") as f:
+        json.dump(res, f, indent=1)
+    print(f"opt_{name}: {len(one)} one-site, {len(two)} two-site values, conditions {conds}")
 
 
 def random_paulis(n, edges, nterms, rng, extra_text=True):
@@ -265,6 +363,20 @@ def main():
             with open(os.path.join(INPUTS, f"rc10x10.{ext}"), "w") as f:
                 f.write(txt)
         run_hostparity("rc10x10", ["qasm", os.path.join(INPUTS, "rc10x10.qasm"), os.path.join(INPUTS, "rc10x10.txt")])
+    if "opttpo" in jobs:
+        q = zz_cx_qasm(3, 3, 2, -0.7, 0.8)  # generic angle: no tie at a rank-1 cut
+        qp = os.path.join(INPUTS, "zzcx3x3.qasm")
+        with open(qp, "w") as f:
+            f.write(q)
+        run_opttpo("zzcx3x3", qp, [1e-8, 1e3])
+        qp = os.path.join(INPUTS, "optmix2x3.qasm")
+        with open(qp, "w") as f:
+            f.write(opt_mix_qasm())
+        run_opttpo("optmix2x3", qp, [1e-8], lattice=(3, 2))
+        run_opttpo("kobe", os.path.join(a.ref, "apps", "estimator", "kicked_ising.qasm"), [1e-8], full=False)
+        orng = np.random.default_rng(20261204)
+        q = zz_cx_qasm(3, 3, 3, -math.pi / 4, 0.7)
+        run_opt_estimator("optzz3x3", q, random_paulis(9, lattice_edges(3), 30, orng), 4, 1e-8, 1e-10, 50, 1e-8)
     if "config1" in jobs:
         run_config1()
 

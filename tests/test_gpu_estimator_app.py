@@ -5,7 +5,7 @@ Run with the reference app's command line on the golden circuits, its printed
 one- and two-site expectation values must equal the reference estimator's
 (the fixtures hold the values the reference printed) to 1e-9, as in
 test_gpu_parity.py's end-to-end test; --precision mixed must stay within
-1e-6 of them.
+1e-6 of them.  The same holds with --do_opt_tpo 1.
 """
 import os
 import re
@@ -23,14 +23,14 @@ ONE = re.compile(r"Expectation value of single site operator at site (\d+) (\S+)
 TWO = re.compile(r"Expectation value of two site operator at sites \((\d+),(\d+)\) (\S+)")
 
 
-def _run(name, meta, precision):
+def _run(name, meta, precision, extra=()):
     if not os.path.exists(APP):
         pytest.fail(f"{APP} is not built: run `python tnbp_b200/build.py`")
     cmd = [APP, "--circuit", os.path.join(HERE, "golden", "inputs", f"{name}.qasm"),
            "--sparse_pauli", os.path.join(HERE, "golden", "inputs", f"{name}.txt"),
            "--max_bond_dim", str(meta["chi"]), "--bp_tolerance", repr(meta["tol"]),
            "--max_bp_iterations", str(meta["maxit"]), "--sv_min", repr(meta["sv_min"]),
-           "--precision", precision, "--sum"]
+           "--precision", precision, "--sum", *extra]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     one = [float(m.group(2)) for m in ONE.finditer(r.stdout)]
@@ -52,3 +52,19 @@ def test_estimator_app_prints_the_reference_values(name, precision, tol):
     for a, b in zip(two, ref_two):
         assert abs(a - b) <= tol, (a, b)
     assert "Sum of c_k <P_k>" in out
+
+
+@pytest.mark.parametrize("precision,tol", [("c128", 1e-9), ("mixed", 1e-6)])
+def test_estimator_app_with_opt_tpo(precision, tol):
+    """--do_opt_tpo 1 (OptTPObySVD on every layer, optsvdtpo.h:86-214): a
+    kicked-Ising circuit with ZZ compiled as cx rz cx; the fixture holds what
+    the reference estimator printed with the same flags."""
+    import json
+    ref = json.load(open(os.path.join(HERE, "golden", "opt_optzz3x3.json")))
+    one, two, out = _run("optzz3x3", ref, precision,
+                         ("--do_opt_tpo", "1", "--eps_opt_tpo", repr(ref["eps_opt_tpo"])))
+    assert out.count("optimization of tpo for layer") == 3
+    assert [int(v) for v in re.findall(r"bond dim = (\d+)", out)] == ref["bond_dims"]
+    assert len(one) == len(ref["one"]) and len(two) == len(ref["two"]), out
+    for a, b in zip(one + two, ref["one"] + ref["two"]):
+        assert abs(a - b) <= tol, (a, b)

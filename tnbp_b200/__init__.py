@@ -56,6 +56,7 @@ _SIGS = {
     "tnbp_qasm_tpo": [C.c_char_p, _i32p, C.c_int64, _i32p, _i64p, _f64p, C.c_int64, _i32p, _i64p],
     "tnbp_kicked_ising_tpo": [_i32p, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double, _i32p, _i64p,
                               _f64p, C.c_int64, _i64p],
+    "tnbp_opt_tpo_svd": [_i32p, C.c_int64, C.c_double, _i32p, _i64p, _f64p, _i64p],
     "tnbp_job_create": [_i32p, C.c_int64, _i32p, C.c_int32, _vp, C.c_uint64, C.POINTER(_vp)],
     "tnbp_job_destroy": [_vp],
     "tnbp_job_info": [_vp, _i64p, _i64p, _i32p],
@@ -289,6 +290,24 @@ def KickedIsingTPO(edges, Jz, hz, hx, dt):
     _chk(lib.tnbp_kicked_ising_tpo(_p(e, _i32p), len(e), Jz, hz, hx, dt, _p(rank, _i32p), _p(off, _i64p),
                                    _p(data, _f64p), nel.value, C.byref(nel)))
     return TPOLayer(rank, off, data.view(np.complex128))
+
+
+def OptTPObySVD(edges, layer, eps=1.0e-8):
+    """OptTPObySVD (optsvdtpo.h:86-214): compress every operator bond of one
+    TPO layer by a truncated SVD (singular values > eps kept), in place as
+    the reference updates its container; returns the layer."""
+    e = _edges_arr(edges)
+    rank = layer.edge_rank.copy()
+    off = layer.op_offset - layer.op_offset.min() if len(layer.op_offset) else layer.op_offset.copy()
+    lo = int(layer.op_offset.min()) if len(layer.op_offset) else 0
+    data = np.ascontiguousarray(layer.op_data[lo:]).view(np.float64).copy()
+    nel = C.c_int64()
+    _chk(lib.tnbp_opt_tpo_svd(_p(e, _i32p), len(e), float(eps), _p(rank, _i32p), _p(off, _i64p),
+                              _p(data, _f64p), C.byref(nel)))
+    layer.edge_rank = rank
+    layer.op_offset = off
+    layer.op_data = data.view(np.complex128)[: nel.value].copy()
+    return layer
 
 
 # ------------------------------------------------------------------ state

@@ -5,15 +5,16 @@
 // Command line as the reference app (apps/estimator/option.h:28-73):
 //   --circuit FILE  --sparse_pauli FILE  --max_bond_dim N  --bp_tolerance X
 //   --max_bp_iterations N  --sv_min X  --truncation_error X (accepted, unused
-//   by the reference too)  --backend default
+//   by the reference too)  --backend default  --do_opt_tpo N (nonzero:
+//   OptTPObySVD on every layer)  --eps_opt_tpo X
 // plus --precision c128|mixed|c64 (default c128, the drop-in) and --sum
 // (print sum_k c_k <P_k>, which the reference does not compute).
 // Printed lines follow the reference's wording for the per-layer BP
 // condition, the per-edge truncation results and the per-term expectation
 // values (one-site terms first, then two-site terms, each in file order);
 // the reference's time stamps are left out.  Not supported here: the
-// ibm_kobe backend's fixed edge list, --num_gates manual layering and
-// --do_opt_tpo (OptTPObySVD), which are outside the BP hot path.
+// ibm_kobe backend's fixed edge list and --num_gates manual layering, which
+// are outside the BP hot path.
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -44,6 +45,8 @@ struct Options {
   std::string backend = "default", circuit = "circuit.qasm", sparsepauli = "sparsepauliop.txt";
   int max_bp_iterations = 50, max_bond_dim = 100;
   double bp_tolerance = 1.0e-8, sv_min = 1.0e-8, truncation_error = 1.0e-8;
+  bool do_opt_tpo = false;
+  double eps_opt_tpo = 1.0e-8;
   int precision = TNBP_C128;
   bool print_sum = false;
 };
@@ -65,13 +68,15 @@ Options parse(int argc, char** argv) {
     else if (a == "--sv_min") o.sv_min = std::atof(next().c_str());
     else if (a == "--truncation_error") o.truncation_error = std::atof(next().c_str());
     else if (a == "--sum") o.print_sum = true;
+    else if (a == "--do_opt_tpo") o.do_opt_tpo = std::atoi(next().c_str()) != 0;
+    else if (a == "--eps_opt_tpo") o.eps_opt_tpo = std::atof(next().c_str());
     else if (a == "--precision") {
       const std::string p = next();
       if (p == "c128") o.precision = TNBP_C128;
       else if (p == "mixed") o.precision = TNBP_MIXED;
       else if (p == "c64") o.precision = TNBP_C64;
       else throw std::invalid_argument("--precision must be c128, mixed or c64");
-    } else if (a == "--num_gates" || a == "--do_opt_tpo" || a == "--eps_opt_tpo") {
+    } else if (a == "--num_gates") {
       throw std::invalid_argument(a + " is not supported by tnbp_estimator");
     }
   }
@@ -111,20 +116,36 @@ int run(const Options& o) {
                       &nelems),
         "tnbp_qasm_tpo");
 
+  // each layer on its own, its offsets re-based to its first element
+  // (tnbp_qasm_tpo packs the layers one after another, site 0 first)
+  std::vector<std::vector<int32_t>> lrank(nlayers);
+  std::vector<std::vector<int64_t>> loff(nlayers);
+  std::vector<std::vector<double>> ldata(nlayers);
+  for (int32_t t = 0; t < nlayers; ++t) {
+    const int64_t base = off[(size_t)t * ns];
+    const int64_t end = t + 1 < nlayers ? off[(size_t)(t + 1) * ns] : nelems;
+    lrank[t].assign(rank.begin() + (size_t)t * ne, rank.begin() + (size_t)(t + 1) * ne);
+    for (int64_t k = 0; k < ns; ++k) loff[t].push_back(off[(size_t)t * ns + k] - base);
+    ldata[t].assign(data.begin() + 2 * base, data.begin() + 2 * end);
+  }
+  if (o.do_opt_tpo) {
+    for (int32_t t = 0; t < nlayers; ++t) {
+      int64_t n = 0;
+      check(tnbp_opt_tpo_svd(edges.data(), ne, o.eps_opt_tpo, lrank[t].data(), loff[t].data(), ldata[t].data(), &n),
+            "tnbp_opt_tpo_svd");
+      ldata[t].resize(2 * n);
+      std::cout << " optimization of tpo for layer " << t << " is performed\n";
+    }
+  }
+
   tnbp_job* job = nullptr;
   check(tnbp_job_create(edges.data(), ne, nullptr, o.precision, nullptr, 0, &job), "tnbp_job_create");
   std::vector<int32_t> dims(ne);
   std::vector<double> errs(ne);
   std::cout.precision(16);
   for (int32_t t = 0; t < nlayers; ++t) {
-    // this layer's operators, re-based to its first element
-    int64_t base = off[(size_t)t * ns];
-    for (int64_t k = 0; k < ns; ++k) base = std::min(base, off[(size_t)t * ns + k]);
-    std::vector<int64_t> loff(ns);
-    for (int64_t k = 0; k < ns; ++k) loff[k] = off[(size_t)t * ns + k] - base;
     tnbp_tpo* tpo = nullptr;
-    check(tnbp_tpo_create(job, rank.data() + (size_t)t * ne, loff.data(), data.data() + 2 * base, &tpo),
-          "tnbp_tpo_create");
+    check(tnbp_tpo_create(job, lrank[t].data(), loff[t].data(), ldata[t].data(), &tpo), "tnbp_tpo_create");
     check(tnbp_absorb_tpo(job, tpo), "tnbp_absorb_tpo");
     check(tnbp_tpo_destroy(tpo), "tnbp_tpo_destroy");
     int32_t iters = 0;

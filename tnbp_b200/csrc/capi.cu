@@ -3,6 +3,7 @@
 // returns the status code; nothing unwinds across the C ABI.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -184,6 +185,39 @@ int tnbp_kicked_ising_tpo(const int32_t* edges, int64_t ne, double Jz, double hz
     auto e = to_edges(edges, ne);
     std::vector<tnbp_host::Layer> layers{tnbp_host::kicked_ising_tpo(e, Jz, hz, hx, dt)};
     put_layers(layers, ne, (int64_t)tnbp_host::site_labels(e).size(), edge_rank, op_offset, op_data, cap, n_elems);
+  });
+}
+
+int tnbp_opt_tpo_svd(const int32_t* edges, int64_t ne, double eps, int32_t* edge_rank, int64_t* op_offset,
+                     double* op_data, int64_t* n_elems) {
+  return guard([&] {
+    need(edge_rank != nullptr && op_offset != nullptr && op_data != nullptr, "NULL argument");
+    auto e = to_edges(edges, ne);
+    const auto bonds_of = [&](int site) { return tnbp_host::surrounding_bonds(e, site); };
+    const auto sites = tnbp_host::site_labels(e);
+    const int64_t ns = (int64_t)sites.size();
+    tnbp_host::Layer L;
+    L.edge_rank.assign(edge_rank, edge_rank + ne);
+    L.op_offset.assign(op_offset, op_offset + ns);
+    int64_t extent = 0;  // elements the input layer spans from op_data[0]
+    for (int64_t s = 0; s < ns; ++s) {
+      int64_t n = 4;
+      for (int m : bonds_of(sites[s])) {
+        need(edge_rank[m] >= 1, "edge_rank < 1");
+        n *= edge_rank[m];
+      }
+      need(op_offset[s] >= 0, "op_offset < 0");
+      extent = std::max(extent, op_offset[s] + n);
+    }
+    L.op_data.assign(op_data, op_data + 2 * extent);
+    tnbp_host::opt_tpo_svd(e, L, eps);
+    // bond dimensions never grow, so a layer packed without overlaps fits
+    const int64_t tot = (int64_t)L.op_data.size() / 2;
+    need(tot <= extent, "op_data too small for the repacked layer (overlapping site operators)");
+    std::copy(L.edge_rank.begin(), L.edge_rank.end(), edge_rank);
+    std::copy(L.op_offset.begin(), L.op_offset.end(), op_offset);
+    std::memcpy(op_data, L.op_data.data(), L.op_data.size() * sizeof(double));
+    if (n_elems) *n_elems = tot;
   });
 }
 

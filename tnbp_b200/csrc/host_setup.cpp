@@ -894,6 +894,123 @@ Layer kicked_ising_tpo(const Edges& edges, double Jz, double hz, double hx, doub
   return pack_layer(lb);
 }
 
+// ------------------------------------------------------ TPO compression
+// OptTPObySVD (include/tnbp/ptns/function/optsvdtpo.h:86-214).  For every
+// edge m = (a, b) in edge order: C = O_a contracted with O_b over their
+// shared bond, rows = O_a's other legs, columns = O_b's other legs (both in
+// leg order, column-major); truncated SVD keeping the singular values
+// > eps, at most the old bond dimension r and at least one; then
+// O_a := U sqrt(s) and O_b := sqrt(s) V^H with the new bond back at the
+// bond's leg position.  C = A B has rank <= r, so its SVD is taken from the
+// factors: A = Ua diag(sa) Vah, W = diag(sa) Vah B = Uw diag(s) Vwh, and
+// C = (Ua Uw) diag(s) Vwh.  The singular values are C's; the singular
+// vectors equal an SVD of C up to a unitary on the bond, which changes no
+// observable; the cost is O((m + n) r^2) instead of O(m n min(m, n)).
+void opt_tpo_svd(const Edges& edges, Layer& layer, double eps) {
+  const auto sites = site_labels(edges);
+  const size_t ns = sites.size(), ne = edges.size();
+  if (layer.edge_rank.size() != ne || layer.op_offset.size() != ns)
+    throw HostError(-1, "TPO layer does not match the edge list");
+  std::map<int, int> pos;
+  for (size_t i = 0; i < ns; ++i) pos[sites[i]] = (int)i;
+  std::vector<std::vector<int>> bonds(ns);
+  for (size_t i = 0; i < ns; ++i) bonds[i] = surrounding_bonds(edges, sites[i]);
+
+  std::vector<SiteOp> ops(ns);
+  const int64_t avail = (int64_t)layer.op_data.size() / 2;
+  for (size_t si = 0; si < ns; ++si) {
+    auto& o = ops[si];
+    int64_t n = 4;
+    for (int m : bonds[si]) {
+      const int r = layer.edge_rank[m];
+      if (r < 1) throw HostError(-1, "TPO bond dimension < 1");
+      o.shape.push_back(r);
+      n *= r;
+    }
+    o.shape.push_back(2);
+    o.shape.push_back(2);
+    const int64_t off = layer.op_offset[si];
+    if (off < 0 || off + n > avail) throw HostError(-1, "TPO site operator outside the op data");
+    o.data.resize(n);
+    for (int64_t x = 0; x < n; ++x) o.data[x] = cd(layer.op_data[2 * (off + x)], layer.op_data[2 * (off + x) + 1]);
+  }
+
+  for (size_t m = 0; m < ne; ++m) {
+    const int ia = pos.at(edges[m].first), ib = pos.at(edges[m].second);
+    const int pa = (int)(std::find(bonds[ia].begin(), bonds[ia].end(), (int)m) - bonds[ia].begin());
+    const int pb = (int)(std::find(bonds[ib].begin(), bonds[ib].end(), (int)m) - bonds[ib].begin());
+    SiteOp& A = ops[ia];
+    SiteOp& B = ops[ib];
+    const int r = A.shape[pa];
+    // A as an (ma x r) matrix, B as an (r x nb) matrix: the row (column)
+    // index is lo + below * hi with lo the legs before the bond, hi after it
+    int64_t below_a = 1, below_b = 1;
+    for (int k = 0; k < pa; ++k) below_a *= A.shape[k];
+    for (int k = 0; k < pb; ++k) below_b *= B.shape[k];
+    const int ma = (int)(A.data.size() / r), nb = (int)(B.data.size() / r);
+    std::vector<cd> Am(A.data.size()), Bm(B.data.size());
+    for (int64_t x = 0; x < (int64_t)A.data.size(); ++x) {
+      const int64_t lo = x % below_a, j = (x / below_a) % r, hi = x / (below_a * r);
+      Am[lo + below_a * hi + (int64_t)ma * j] = A.data[x];
+    }
+    for (int64_t x = 0; x < (int64_t)B.data.size(); ++x) {
+      const int64_t lo = x % below_b, j = (x / below_b) % r, hi = x / (below_b * r);
+      Bm[j + (int64_t)r * (lo + below_b * hi)] = B.data[x];
+    }
+    std::vector<cd> Ua, Vah, Uw, Vwh;
+    std::vector<double> sa, sw;
+    small_svd(ma, r, Am, Ua, sa, Vah);
+    const int ka = (int)sa.size();
+    std::vector<cd> W((size_t)ka * nb, 0.0);
+    for (int c = 0; c < nb; ++c)
+      for (int j = 0; j < r; ++j) {
+        const cd b = Bm[j + (size_t)r * c];
+        if (b == 0.0) continue;
+        for (int i = 0; i < ka; ++i) W[i + (size_t)ka * c] += sa[i] * Vah[i + (size_t)ka * j] * b;
+      }
+    small_svd(ka, nb, W, Uw, sw, Vwh);
+    const int kw = (int)sw.size();
+    int keep = 0;
+    while (keep < kw && keep < r && sw[keep] > eps) ++keep;
+    if (keep == 0) keep = 1;
+
+    SiteOp nA, nB;
+    nA.shape = A.shape;
+    nA.shape[pa] = keep;
+    nB.shape = B.shape;
+    nB.shape[pb] = keep;
+    nA.data.assign((size_t)ma * keep, 0.0);
+    nB.data.assign((size_t)nb * keep, 0.0);
+    for (int j = 0; j < keep; ++j) {
+      const double sq = std::sqrt(sw[j]);
+      for (int row = 0; row < ma; ++row) {
+        cd u = 0;  // (Ua Uw)[row, j]
+        for (int i = 0; i < ka; ++i) u += Ua[row + (size_t)ma * i] * Uw[i + (size_t)ka * j];
+        const int64_t lo = row % below_a, hi = row / below_a;
+        nA.data[lo + below_a * (j + (int64_t)keep * hi)] = u * sq;
+      }
+      for (int col = 0; col < nb; ++col) {
+        const int64_t lo = col % below_b, hi = col / below_b;
+        nB.data[lo + below_b * (j + (int64_t)keep * hi)] = sq * Vwh[j + (size_t)kw * col];
+      }
+    }
+    A = std::move(nA);
+    B = std::move(nB);
+  }
+
+  Layer out;
+  out.edge_rank.assign(ne, 1);
+  for (size_t si = 0; si < ns; ++si)
+    for (size_t k = 0; k < bonds[si].size(); ++k) out.edge_rank[bonds[si][k]] = ops[si].shape[k];
+  int64_t off = 0;
+  for (size_t si = 0; si < ns; ++si) {
+    out.op_offset.push_back(off);
+    for (auto& v : ops[si].data) { out.op_data.push_back(v.real()); out.op_data.push_back(v.imag()); }
+    off += (int64_t)ops[si].data.size();
+  }
+  layer = std::move(out);
+}
+
 // -------------------------------------------------------------- Pauli
 // load_sparse_pauli_op (sparse_pauli.h:52-97) on text; classification of
 // ClassifyOps (paulitotpo.h:99-153).

@@ -48,6 +48,7 @@ int qubit_count(const Instruction& in);
 Edges qasm_edges(const Program& p);
 std::vector<Layer> qasm_tpo(const Program& p, const Edges& edges);
 Layer kicked_ising_tpo(const Edges& edges, double Jz, double hz, double hx, double dt);
+void opt_tpo_svd(const Edges& edges, Layer& layer, double eps);
 std::vector<PauliTerm> pauli_terms(const std::string& text, const Edges& edges, int64_t* n_dropped);
 std::vector<std::complex<double>> pauli_list(char letter);
 
