@@ -171,6 +171,41 @@ int tnbp_download_message(tnbp_job* job, int64_t m, double* data, int64_t cap_el
    edge's bond dimension before the next device call. */
 int tnbp_upload_message(tnbp_job* job, int64_t m, int32_t dim, const double* data);
 
+/* ============================== checkpoints ============================== */
+/* Files in the layout of SaveTPS / LoadTPS
+   (include/tnbp/ptns/function/iotps.h:37-105, apps/estimator_restart):
+   size_t |V|, |Site_To_MpiRank|, |EdgeIdx|; the site tensors; SiteIdx; the
+   (site, rank) pairs; the 2|EdgeIdx| messages; EdgeIdx.  Each tensor is
+   uint64 order, int32 shape[order], complex128 scale (1), complex128 data
+   column-major -- the record of gqten::tensor<std::complex<double>>::
+   StreamWrite as restated for the reference's CPU build (gqten itself is not
+   available).  These calls handle the whole state of one edge list held by
+   one rank (every site on rank 0, EdgeIdx = 0 .. n_edges-1); a file written
+   by one rank of several is rejected (TNBP_EINVAL). */
+
+/* SaveTPS from host arrays: site tensors packed in sorted-site order, each of
+   shape (bond_dim of its legs in leg order..., phys), then the 2*n_edges
+   messages packed in order, message m of shape (bond_dim[m % n_edges])^2;
+   complex128 interleaved.  phys_dims may be NULL (all 2). */
+int tnbp_tps_write(const char* path, const int32_t* edges, int64_t n_edges, const int32_t* bond_dim,
+                   const int32_t* phys_dims, const double* site_data, const double* msg_data);
+/* LoadTPS into host arrays in the layout of tnbp_tps_write, after checking
+   that the file holds the whole state of `edges` (site labels, edge ids,
+   orders, shapes that agree on every bond).  Any output may be NULL;
+   site_elems_out / msg_elems_out give the complex element counts. */
+int tnbp_tps_read(const char* path, const int32_t* edges, int64_t n_edges, int32_t* bond_dim,
+                  int32_t* phys_dims, double* site_data, int64_t site_cap, double* msg_data,
+                  int64_t msg_cap, int64_t* site_elems_out, int64_t* msg_elems_out);
+/* SaveTPS of a job's current site tensors and messages (the restart app's
+   save after its last step, apps/estimator_restart/main.cc:253-257).  The
+   file holds complex128 whatever the job's precision. */
+int tnbp_save_state(tnbp_job* job, const char* path);
+/* LoadTPS into a job created on the same edge list and physical dimensions
+   (apps/estimator_restart/main.cc:84-92): bond dimensions, site tensors and
+   messages are replaced.  A file that does not match leaves the job as it
+   was; if device memory runs out after the check, destroy the job. */
+int tnbp_load_state(tnbp_job* job, const char* path);
+
 /* A TPO layer resident on the device (layout of tnbp_qasm_tpo, one layer). */
 int tnbp_tpo_create(tnbp_job* job, const int32_t* edge_rank, const int64_t* op_offset,
                     const double* op_data, tnbp_tpo** out);

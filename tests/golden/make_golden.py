@@ -19,6 +19,10 @@ oracle/_ref/, and this script runs them on seeded synthetic inputs:
                      to gauge-invariant data (bond dimensions, per-leg
                      singular values of every site operator)
   opt_<name>.json    the estimator app's printed values with --do_opt_tpo 1
+  ckpt_<name>000000.dat + ckpt_<name>.json
+                     a checkpoint the reference's estimator_restart app saved
+                     after one pass of a circuit (SaveTPS, iotps.h) and the
+                     values it printed after a second pass loaded from it
   config1.json       observables of the 4x4 kicked-Ising workload from the
                      reference apps kicked_ising_lattice and estimator
 
@@ -194,6 +198,29 @@ def run_opt_estimator(name, qasm, pauli, chi, sv_min, tol, maxit, eps):
     with open(os.path.join(HERE, f"opt_{name}.json"), "w") as f:
         json.dump(res, f, indent=1)
     print(f"opt_{name}: {len(one)} one-site, {len(two)} two-site values, conditions {conds}")
+
+
+def run_checkpoint(name, qasm, pauli, chi, sv_min, tol, maxit, nlayers):
+    qp = os.path.join(INPUTS, f"{name}.qasm")
+    pp = os.path.join(INPUTS, f"{name}.txt")
+    with open(qp, "w") as f:
+        f.write(qasm)
+    with open(pp, "w") as f:
+        f.write(pauli)
+    app = os.path.join(REF_BIN, "estimator_restart")
+    base = [app, "--circuit", qp, "--sparse_pauli", pp, "--max_bond_dim", str(chi), "--bp_tolerance", repr(tol),
+            "--max_bp_iterations", str(maxit), "--sv_min", repr(sv_min)]
+    prefix = os.path.join(HERE, f"ckpt_{name}")
+    subprocess.check_output(base + ["--step_end", "1", "--savename", prefix], text=True)
+    out = subprocess.check_output(base + ["--loadname", prefix, "--step_start", "1", "--step_end", "2",
+                                          "--measurement_barrier", str(nlayers - 1)], text=True)
+    one = [float(v) for v in re.findall(r"single site operator for step 1 barrier \d+ at site \d+ (\S+)", out)]
+    two = [float(v) for v in re.findall(r"two site operator for step 1 barrier \d+ at sites \(\d+,\d+\) (\S+)", out)]
+    dims = [int(v) for v in re.findall(r"bond dim = (\d+)", out)]
+    res = dict(chi=chi, sv_min=sv_min, tol=tol, maxit=maxit, one=one, two=two, bond_dims=dims)
+    with open(os.path.join(HERE, f"ckpt_{name}.json"), "w") as f:
+        json.dump(res, f, indent=1)
+    print(f"ckpt_{name}: {len(one)} one-site, {len(two)} two-site values after the restart")
 
 
 def random_paulis(n, edges, nterms, rng, extra_text=True):
@@ -377,6 +404,10 @@ def main():
         orng = np.random.default_rng(20261204)
         q = zz_cx_qasm(3, 3, 3, -math.pi / 4, 0.7)
         run_opt_estimator("optzz3x3", q, random_paulis(9, lattice_edges(3), 30, orng), 4, 1e-8, 1e-10, 50, 1e-8)
+    if "ckpt" in jobs:
+        crng = np.random.default_rng(20261205)
+        q = kicked_ising_qasm(3, 3, 3, -0.8, 0.6)
+        run_checkpoint("ki3x3r", q, random_paulis(9, lattice_edges(3), 30, crng), 4, 1e-8, 1e-10, 50, 3)
     if "config1" in jobs:
         run_config1()
 

@@ -57,6 +57,11 @@ _SIGS = {
     "tnbp_kicked_ising_tpo": [_i32p, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double, _i32p, _i64p,
                               _f64p, C.c_int64, _i64p],
     "tnbp_opt_tpo_svd": [_i32p, C.c_int64, C.c_double, _i32p, _i64p, _f64p, _i64p],
+    "tnbp_tps_write": [C.c_char_p, _i32p, C.c_int64, _i32p, _i32p, _f64p, _f64p],
+    "tnbp_tps_read": [C.c_char_p, _i32p, C.c_int64, _i32p, _i32p, _f64p, C.c_int64, _f64p, C.c_int64, _i64p,
+                      _i64p],
+    "tnbp_save_state": [_vp, C.c_char_p],
+    "tnbp_load_state": [_vp, C.c_char_p],
     "tnbp_job_create": [_i32p, C.c_int64, _i32p, C.c_int32, _vp, C.c_uint64, C.POINTER(_vp)],
     "tnbp_job_destroy": [_vp],
     "tnbp_job_info": [_vp, _i64p, _i64p, _i32p],
@@ -310,6 +315,48 @@ def OptTPObySVD(edges, layer, eps=1.0e-8):
     return layer
 
 
+def SaveTPS(path, edges, V, E):
+    """SaveTPS (iotps.h:37-67) of a whole single-rank state held on the host:
+    V[s] site tensors in sorted-site order, E[m] the 2|E| messages."""
+    e = _edges_arr(edges)
+    sites = GetSiteIndexFromBond(edges)
+    bond = np.array([np.asarray(E[m]).shape[0] for m in range(len(e))], np.int32)
+    phys = np.array([np.asarray(v).shape[-1] for v in V], np.int32)
+    vdata = np.concatenate([_c128(v).reshape(-1, order="F") for v in V]) if len(sites) else np.zeros(1, np.complex128)
+    mdata = np.concatenate([_c128(x).reshape(-1, order="F") for x in E]) if len(e) else np.zeros(1, np.complex128)
+    _chk(lib.tnbp_tps_write(os.fsencode(path), _p(e, _i32p), len(e), _p(bond, _i32p), _p(phys, _i32p),
+                            _p(vdata.view(np.float64), _f64p), _p(mdata.view(np.float64), _f64p)))
+
+
+def LoadTPS(path, edges):
+    """LoadTPS (iotps.h:69-105) of a whole single-rank checkpoint of `edges`:
+    returns (V, E) as lists of complex128 arrays."""
+    e = _edges_arr(edges)
+    sites = GetSiteIndexFromBond(edges)
+    bond = np.zeros(max(1, len(e)), np.int32)
+    phys = np.zeros(max(1, len(sites)), np.int32)
+    nv, nm = C.c_int64(), C.c_int64()
+    s = os.fsencode(path)
+    _chk(lib.tnbp_tps_read(s, _p(e, _i32p), len(e), None, None, None, 0, None, 0, C.byref(nv), C.byref(nm)))
+    vdata = np.zeros(max(1, nv.value), np.complex128)
+    mdata = np.zeros(max(1, nm.value), np.complex128)
+    _chk(lib.tnbp_tps_read(s, _p(e, _i32p), len(e), _p(bond, _i32p), _p(phys, _i32p),
+                           _p(vdata.view(np.float64), _f64p), nv.value, _p(mdata.view(np.float64), _f64p), nm.value,
+                           C.byref(nv), C.byref(nm)))
+    V, o = [], 0
+    for si, site in enumerate(sites):
+        shape = [int(bond[m]) for m in GetSurroundingBondIndex(site, edges)] + [int(phys[si])]
+        n = int(np.prod(shape))
+        V.append(vdata[o:o + n].reshape(shape, order="F").copy())
+        o += n
+    E, o = [], 0
+    for m in range(2 * len(e)):
+        D = int(bond[m % len(e)])
+        E.append(mdata[o:o + D * D].reshape((D, D), order="F").copy())
+        o += D * D
+    return V, E
+
+
 # ------------------------------------------------------------------ state
 class State:
     """Device-resident PEPS of one job (site tensors and both message
@@ -411,6 +458,14 @@ class State:
                                  _p(layer.op_data.view(np.float64), _f64p), C.byref(t)))
         self._tpos.append(t)
         return t
+
+    def save(self, path):
+        """SaveTPS of the device state (tnbp_save_state)."""
+        _chk(lib.tnbp_save_state(self.h, os.fsencode(path)))
+
+    def load(self, path):
+        """LoadTPS into this job (tnbp_load_state)."""
+        _chk(lib.tnbp_load_state(self.h, os.fsencode(path)))
 
     def sweep_stats(self):
         ms, fl, by = C.c_double(), C.c_double(), C.c_double()

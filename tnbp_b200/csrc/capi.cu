@@ -14,6 +14,7 @@
 #include "engine.h"
 #include "host_setup.h"
 #include "server.h"
+#include "tps_io.h"
 
 using tnbp::Error;
 
@@ -218,6 +219,106 @@ int tnbp_opt_tpo_svd(const int32_t* edges, int64_t ne, double eps, int32_t* edge
     std::copy(L.op_offset.begin(), L.op_offset.end(), op_offset);
     std::memcpy(op_data, L.op_data.data(), L.op_data.size() * sizeof(double));
     if (n_elems) *n_elems = tot;
+  });
+}
+
+// ----------------------------------------------------------- checkpoints
+int tnbp_tps_write(const char* path, const int32_t* edges, int64_t ne, const int32_t* bond_dim,
+                   const int32_t* phys_dims, const double* site_data, const double* msg_data) {
+  return guard([&] {
+    need(path && bond_dim && site_data && msg_data, "NULL argument");
+    auto e = to_edges(edges, ne);
+    const size_t ns = tnbp_host::site_labels(e).size();
+    std::vector<int> bd(bond_dim, bond_dim + ne), pd(ns, 2);
+    if (phys_dims) pd.assign(phys_dims, phys_dims + ns);
+    for (int d : bd) need(d >= 1, "bond dimension < 1");
+    for (int d : pd) need(d >= 1, "physical dimension < 1");
+    tnbp_host::tps_write(path, tnbp_host::tps_whole(e, bd, pd, reinterpret_cast<const std::complex<double>*>(site_data),
+                                                    reinterpret_cast<const std::complex<double>*>(msg_data)));
+  });
+}
+
+int tnbp_tps_read(const char* path, const int32_t* edges, int64_t ne, int32_t* bond_dim, int32_t* phys_dims,
+                  double* site_data, int64_t site_cap, double* msg_data, int64_t msg_cap, int64_t* site_elems,
+                  int64_t* msg_elems) {
+  return guard([&] {
+    need(path != nullptr, "path is NULL");
+    auto e = to_edges(edges, ne);
+    const auto st = tnbp_host::tps_read(path);
+    std::vector<int> bd, pd;
+    tnbp_host::tps_check_whole(st, e, bd, pd);
+    int64_t nv = 0, nm = 0;
+    for (const auto& t : st.V) nv += (int64_t)t.data.size();
+    for (const auto& t : st.E) nm += (int64_t)t.data.size();
+    if (site_elems) *site_elems = nv;
+    if (msg_elems) *msg_elems = nm;
+    if (bond_dim) std::copy(bd.begin(), bd.end(), bond_dim);
+    if (phys_dims) std::copy(pd.begin(), pd.end(), phys_dims);
+    if (site_data) {
+      need(site_cap >= nv, "site_data capacity too small");
+      int64_t o = 0;
+      for (const auto& t : st.V) {
+        std::memcpy(site_data + 2 * o, t.data.data(), t.data.size() * 16);
+        o += (int64_t)t.data.size();
+      }
+    }
+    if (msg_data) {
+      need(msg_cap >= nm, "msg_data capacity too small");
+      int64_t o = 0;
+      for (const auto& t : st.E) {
+        std::memcpy(msg_data + 2 * o, t.data.data(), t.data.size() * 16);
+        o += (int64_t)t.data.size();
+      }
+    }
+  });
+}
+
+int tnbp_save_state(tnbp_job* job, const char* path) {
+  return guard([&] {
+    need(job && path, "NULL argument");
+    auto& J = *job->j;
+    const size_t ns = J.g.labels.size(), ne = J.g.edges.size();
+    std::vector<double> hv(2 * J.v_elems), hm(2 * J.m_elems);
+    J.get_complex(J.V, hv.data(), J.v_elems, 0);
+    J.get_complex(J.M[J.cur], hm.data(), J.m_elems, 0);
+    std::vector<double> sv, mv;
+    for (size_t s = 0; s < ns; ++s)
+      sv.insert(sv.end(), hv.begin() + 2 * J.voff[s], hv.begin() + 2 * (J.voff[s] + J.site_elems((int)s)));
+    for (size_t m = 0; m < 2 * ne; ++m) {
+      const size_t dd = (size_t)J.dim[m % ne] * J.dim[m % ne];
+      mv.insert(mv.end(), hm.begin() + 2 * J.moff[m], hm.begin() + 2 * (J.moff[m] + dd));
+    }
+    tnbp_host::tps_write(path, tnbp_host::tps_whole(J.g.edges, J.dim, J.pd,
+                                                    reinterpret_cast<const std::complex<double>*>(sv.data()),
+                                                    reinterpret_cast<const std::complex<double>*>(mv.data())));
+  });
+}
+
+int tnbp_load_state(tnbp_job* job, const char* path) {
+  return guard([&] {
+    need(job && path, "NULL argument");
+    auto& J = *job->j;
+    const auto st = tnbp_host::tps_read(path);
+    std::vector<int> bd, pd;
+    tnbp_host::tps_check_whole(st, J.g.edges, bd, pd);
+    need(pd == J.pd, "checkpoint physical dimensions differ from the job's");
+    J.dim = bd;
+    J.layout();
+    J.V.alloc(J.v_elems * J.esz, J.stream);
+    J.M[0].alloc(J.m_elems * J.esz, J.stream);
+    J.M[1].alloc(J.m_elems * J.esz, J.stream);
+    J.check_budget();
+    std::vector<double> hv(2 * J.v_elems, 0.0), hm(2 * J.m_elems, 0.0);
+    for (size_t s = 0; s < st.V.size(); ++s)
+      std::memcpy(hv.data() + 2 * J.voff[s], st.V[s].data.data(), st.V[s].data.size() * 16);
+    for (size_t m = 0; m < st.E.size(); ++m)
+      std::memcpy(hm.data() + 2 * J.moff[m], st.E[m].data.data(), st.E[m].data.size() * 16);
+    J.put_complex(J.V, hv.data(), J.v_elems, 0);
+    J.put_complex(J.M[0], hm.data(), J.m_elems, 0);
+    J.cur = 0;
+    J.shadow_dirty = true;
+    J.destroy_graphs();
+    J.plan = tnbp::SweepPlan();
   });
 }
 
