@@ -328,6 +328,24 @@ int tnbp_server_submit_kicked_ising(tnbp_server* srv, int32_t L, int32_t chi, in
                                     const int32_t* kind, const int32_t* q0, const int32_t* q1,
                                     const char* letters, const double* coeff,
                                     int64_t* request_id);
+/* Queue an estimator request for a QASM program and a sparse-Pauli
+   observable (the estimator app's workload, apps/estimator/main.cc:105-238):
+   edges = EdgesFromQasm, one TPO layer per barrier block (QasmToTPO), each
+   compressed by OptTPObySVD when do_opt_tpo != 0; then per layer AbsorbTPO,
+   the BP loop and Truncation to chi; finally the terms ClassifyOps keeps are
+   measured and summed (Σ c_k <P_k>).  The TPO layers of a program are built
+   and uploaded once and shared on the device by every request with the same
+   program text and TPO options (least-recently-used cache of 32 programs;
+   kicked-Ising requests are cached by (L, theta_j, theta_h) the same way).
+   Parse errors return TNBP_EPARSE; a one-site term on a qubit that no
+   two-qubit gate touches, TNBP_EINVAL. */
+int tnbp_server_submit_qasm(tnbp_server* srv, const char* qasm_src, const char* pauli_text,
+                            int32_t chi, double bp_tol, int32_t bp_max_iter, double sv_min,
+                            int32_t do_opt_tpo, double eps_opt_tpo, int64_t* request_id);
+/* TPO cache counters: look-ups served from the cache, layers built, and the
+   programs held now. */
+int tnbp_server_tpo_cache_stats(tnbp_server* srv, int64_t* hits_out, int64_t* misses_out,
+                                int64_t* entries_out);
 /* Advance the loop once (admission + one batched stage).  n_done_out =
    number of requests that completed during this call. */
 int tnbp_server_step(tnbp_server* srv, int32_t* n_active_out, int32_t* n_queued_out,

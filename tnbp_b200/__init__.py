@@ -89,6 +89,9 @@ _SIGS = {
     "tnbp_server_submit_kicked_ising": [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                         C.c_double, C.c_int32, C.c_double, C.c_int64, _i32p, _i32p, _i32p,
                                         C.c_char_p, _f64p, _i64p],
+    "tnbp_server_submit_qasm": [_vp, C.c_char_p, C.c_char_p, C.c_int32, C.c_double, C.c_int32, C.c_double,
+                                C.c_int32, C.c_double, _i64p],
+    "tnbp_server_tpo_cache_stats": [_vp, _i64p, _i64p, _i64p],
     "tnbp_server_step": [_vp, _i32p, _i32p, _i32p],
     "tnbp_server_result": [_vp, C.c_int64, _f64p, _i32p],
 }
@@ -573,6 +576,20 @@ class Server:
                                                  terms.letters if n else b"II", _p(co.view(np.float64), _f64p),
                                                  C.byref(rid)))
         return rid.value
+
+    def submit_qasm(self, qasm_src, pauli_text, chi, bp_tol=1e-8, bp_max_iter=50, sv_min=1e-8, do_opt_tpo=False,
+                    eps_opt_tpo=1e-8):
+        """The estimator app's workload as a served request: returns its id."""
+        rid = C.c_int64()
+        _chk(lib.tnbp_server_submit_qasm(self.h, qasm_src.encode(), pauli_text.encode(), chi, bp_tol, bp_max_iter,
+                                         sv_min, 1 if do_opt_tpo else 0, eps_opt_tpo, C.byref(rid)))
+        return rid.value
+
+    def tpo_cache_stats(self):
+        """(hits, misses, entries) of the server's TPO cache."""
+        h, m, e = C.c_int64(), C.c_int64(), C.c_int64()
+        _chk(lib.tnbp_server_tpo_cache_stats(self.h, C.byref(h), C.byref(m), C.byref(e)))
+        return h.value, m.value, e.value
 
     def step(self):
         a, q, d = C.c_int32(), C.c_int32(), C.c_int32()

@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 
 #include "../../include/tnbp_b200.h"
@@ -50,39 +51,110 @@ Server::Server(int precision, uint64_t budget_bytes, int max_active_jobs)
 
 Server::~Server() {
   batch = SweepBatch();
-  for (auto& kv : reqs) { kv.second->job.reset(); kv.second->tpo.reset(); }
+  for (auto& kv : reqs) { kv.second->job.reset(); kv.second->tpos.reset(); }
+  tpo_cache.clear();
   if (hcond) cudaFreeHost(hcond);
   if (stream) { cudaStreamSynchronize(stream); cudaStreamDestroy(stream); }
 }
 
-// Peak device bytes of a kicked-Ising request on an L x L lattice: BP runs
-// at bond dimension 2*chi; per site the tensor, its spare buffer, the two
-// chain buffers of truncation, the complex64 sweep copy (TNBP_MIXED) and the
-// sweep scratch slots of its degree; both message arenas twice; per-edge
-// truncation work.
+// Sweep scratch slots of a degree-g site under the tree schedule of
+// Job::build_plan: S(1) = 0, S(n) = n + S(n/2) + S(n - n/2).
+static int sweep_slots(int g) {
+  if (g <= 1) return 0;
+  const int h = g / 2;
+  return g + sweep_slots(h) + sweep_slots(g - h);
+}
+
+// Peak device bytes of a request.  Bond dimension during BP on edge e: at
+// most chi times the largest TPO rank on e, and at most the product of the
+// ranks absorbed since |0...0>.  Per site the tensor, its spare buffer, the
+// two chain buffers of truncation, the complex64 sweep copy (TNBP_MIXED) and
+// the sweep scratch slots of its degree; both message arenas twice; per-edge
+// truncation work and Gram partials; the request's TPO layers.
 uint64_t Server::footprint(const Request& r) const {
   const double esz = prec == TNBP_C64 ? 8.0 : 16.0;   // stored element
   const double wsz = prec == TNBP_C128 ? 16.0 : 8.0;  // sweep element
   const double shadow = prec == TNBP_MIXED ? 8.0 : 0.0;
-  const double D = 2.0 * r.chi;
-  const int L = r.L;
-  double bytes = 0.0;
-  for (int y = 0; y < L; ++y)
-    for (int x = 0; x < L; ++x) {
-      const int g = (x > 0) + (x < L - 1) + (y > 0) + (y < L - 1);
-      const int slots = g == 4 ? 8 : g == 3 ? 5 : g == 2 ? 2 : 0;
-      const double n = 2.0 * std::pow(D, g);
-      bytes += n * (4.0 * esz + shadow + wsz * slots);  // V, spare, 2 chain buffers
+  const TpoSet& ts = *r.tpos;
+  const auto& edges = ts.edges;
+  const size_t ne = edges.size();
+  const int nsteps = r.source == Request::QASM ? (int)ts.layers.size() : r.steps;
+  std::vector<double> D(ne);
+  for (size_t e = 0; e < ne; ++e) {
+    const double cap = (double)r.chi * ts.rank_max[e];
+    double prod = 1.0;
+    for (int t = 0; t < nsteps && prod < cap; ++t)
+      prod *= ts.layers[r.source == Request::QASM ? t : 0]->rank[e];
+    D[e] = std::max(1.0, std::min(cap, prod));
+  }
+  const auto sites = tnbp_host::site_labels(edges);
+  std::map<int, size_t> pos;
+  for (size_t i = 0; i < sites.size(); ++i) pos[sites[i]] = i;
+  std::vector<double> n(sites.size(), 2.0);  // elements of each site tensor
+  std::vector<int> deg(sites.size(), 0);
+  for (size_t e = 0; e < ne; ++e)
+    for (int v : {edges[e].first, edges[e].second}) {
+      n[pos[v]] *= D[e];
+      ++deg[pos[v]];
     }
-  const double ne = 2.0 * L * (L - 1);
-  bytes += 4.0 * 2.0 * ne * D * D * esz;      // message arenas (old + new)
-  bytes += ne * 8.0 * D * D * 16.0;           // truncation work
-  bytes += 2.0 * ne * 16.0 * D * D * 16.0;    // Gram partials (upper bound)
+  double bytes = 0.0;
+  for (size_t i = 0; i < sites.size(); ++i)
+    bytes += n[i] * (4.0 * esz + shadow + wsz * sweep_slots(deg[i]));  // V, spare, 2 chain buffers
+  for (size_t e = 0; e < ne; ++e) {
+    const double dd = D[e] * D[e];
+    bytes += 4.0 * 2.0 * dd * esz;   // message arenas (old + new)
+    bytes += 8.0 * dd * 16.0;        // truncation work
+    bytes += 2.0 * 16.0 * dd * 16.0; // Gram partials (upper bound)
+  }
+  bytes += (double)ts.device_bytes;
   return (uint64_t)(bytes * 1.1) + (8ull << 20);
 }
 
+// The TPO layers of a circuit, built and uploaded on the first request that
+// names it and shared with every later one while it stays in the cache.
+std::shared_ptr<const TpoSet> Server::tpo_set(
+    const std::string& key,
+    const std::function<void(tnbp_host::Edges&, std::vector<tnbp_host::Layer>&)>& build) {
+  auto it = tpo_cache.find(key);
+  if (it != tpo_cache.end()) {
+    ++cache_hits;
+    tpo_lru.remove(key);
+    tpo_lru.push_back(key);
+    return it->second;
+  }
+  ++cache_misses;
+  TNBP_TRACE_SCOPE("server.tpo_build");
+  auto ts = std::make_shared<TpoSet>();
+  std::vector<tnbp_host::Layer> layers;
+  build(ts->edges, layers);
+  if (ts->edges.empty()) throw Error(TNBP_EINVAL, "the circuit has no two-qubit gate (no edges)");
+  const size_t ne = ts->edges.size(), ns = tnbp_host::site_labels(ts->edges).size();
+  ts->rank_max.assign(ne, 1);
+  for (const auto& L : layers) {
+    auto t = std::make_unique<Tpo>();
+    t->rank.assign(L.edge_rank.begin(), L.edge_rank.end());
+    for (size_t e = 0; e < ne; ++e) ts->rank_max[e] = std::max(ts->rank_max[e], t->rank[e]);
+    t->op_offset = L.op_offset;
+    t->dout.assign(ns, 2);
+    t->ops.alloc(L.op_data.size() * sizeof(double), stream);
+    CK(cudaMemcpyAsync(t->ops.p, L.op_data.data(), L.op_data.size() * sizeof(double), cudaMemcpyHostToDevice,
+                       stream));
+    ts->device_bytes += L.op_data.size() * sizeof(double);
+    ts->layers.push_back(std::move(t));
+  }
+  CK(cudaStreamSynchronize(stream));
+  tpo_cache[key] = ts;
+  tpo_lru.push_back(key);
+  while (tpo_cache.size() > tpo_cache_cap) {
+    tpo_cache.erase(tpo_lru.front());
+    tpo_lru.pop_front();
+  }
+  return ts;
+}
+
 int64_t Server::submit(std::unique_ptr<Request> r) {
-  if (r->L < 2) throw Error(TNBP_EINVAL, "lattice side must be >= 2");
+  if (!r->tpos) throw Error(TNBP_EINVAL, "request without TPO layers");
+  if (r->source == Request::KICKED_ISING && r->L < 2) throw Error(TNBP_EINVAL, "lattice side must be >= 2");
   if (r->chi < 1 || r->steps < 0 || r->maxit < 0) throw Error(TNBP_EINVAL, "bad request parameters");
   r->footprint = footprint(*r);
   if (r->footprint > budget) throw Error(TNBP_ENOMEM, "request footprint exceeds the server's HBM budget");
@@ -94,21 +166,10 @@ int64_t Server::submit(std::unique_ptr<Request> r) {
 }
 
 void Server::start(Request& r) {
-  const auto edges = tnbp_host::square_lattice(r.L, r.L);
+  const auto& edges = r.tpos->edges;
   std::vector<int32_t> e(2 * edges.size());
   for (size_t i = 0; i < edges.size(); ++i) { e[2 * i] = edges[i].first; e[2 * i + 1] = edges[i].second; }
   r.job = std::make_unique<Job>(e.data(), (int64_t)edges.size(), nullptr, prec, stream, 0);
-  // RZZ(theta_j) = exp(-i theta_j/2 ZZ), RX(theta_h) = exp(-i theta_h/2 X)
-  const auto layer = tnbp_host::kicked_ising_tpo(edges, r.theta_j / 2.0, 0.0, r.theta_h / 2.0, 1.0);
-  auto t = std::make_unique<Tpo>();
-  t->rank.assign(layer.edge_rank.begin(), layer.edge_rank.end());
-  t->op_offset = layer.op_offset;
-  t->dout.assign(r.job->g.labels.size(), 2);
-  t->ops.alloc(layer.op_data.size() * sizeof(double), stream);
-  CK(cudaMemcpyAsync(t->ops.p, layer.op_data.data(), layer.op_data.size() * sizeof(double), cudaMemcpyHostToDevice,
-                     stream));
-  CK(cudaStreamSynchronize(stream));
-  r.tpo = std::move(t);
   r.step = 0;
   r.phase = r.steps > 0 ? Request::ABSORB : Request::MEASURE;
 }
@@ -146,7 +207,7 @@ void Server::finish(Request& r) {
   }
   r.job->measure_terms(terms, nullptr, r.result);
   r.job.reset();
-  r.tpo.reset();
+  r.tpos.reset();
   r.phase = Request::DONE;
 }
 
@@ -158,7 +219,7 @@ void Server::fail(Request& r, int code, const std::string& msg) {
   r.error = msg;
   r.result[0] = r.result[1] = std::nan("");
   r.job.reset();
-  r.tpo.reset();
+  r.tpos.reset();
   r.phase = Request::DONE;
 }
 
@@ -179,7 +240,7 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
   for (int64_t id : active) {
     Request& r = *reqs[id];
     if (r.phase == Request::ABSORB) {
-      r.job->absorb_tpo(*r.tpo);
+      r.job->absorb_tpo(*r.tpos->layers[r.source == Request::QASM ? r.step : 0]);
       r.phase = Request::BP;
       r.bp_iters = 0;
       r.prev_cond = INFINITY;
@@ -319,8 +380,65 @@ int tnbp_server_submit_kicked_ising(tnbp_server* srv, int32_t L, int32_t chi, in
     r->coeff.assign(coeff, coeff + 2 * n_terms);
     for (int64_t i = 0; i < n_terms; ++i)
       if (r->kind[i] != 1 && r->kind[i] != 2) throw tnbp::Error(TNBP_EINVAL, "term kind must be 1 or 2");
+    if (L < 2) throw tnbp::Error(TNBP_EINVAL, "lattice side must be >= 2");
+    // RZZ(theta_j) = exp(-i theta_j/2 ZZ), RX(theta_h) = exp(-i theta_h/2 X)
+    char key[96];
+    std::snprintf(key, sizeof(key), "kicked_ising %d %a %a", L, theta_j, theta_h);
+    r->tpos = srv->s->tpo_set(key, [&](tnbp_host::Edges& e, std::vector<tnbp_host::Layer>& layers) {
+      e = tnbp_host::square_lattice(L, L);
+      layers.push_back(tnbp_host::kicked_ising_tpo(e, theta_j / 2.0, 0.0, theta_h / 2.0, 1.0));
+    });
     const int64_t id = srv->s->submit(std::move(r));
     if (request_id) *request_id = id;
+  });
+}
+
+int tnbp_server_submit_qasm(tnbp_server* srv, const char* qasm_src, const char* pauli_text, int32_t chi,
+                            double bp_tol, int32_t bp_max_iter, double sv_min, int32_t do_opt_tpo,
+                            double eps_opt_tpo, int64_t* request_id) {
+  return sguard([&] {
+    if (!srv) throw tnbp::Error(TNBP_EINVAL, "server is NULL");
+    if (!qasm_src || !pauli_text) throw tnbp::Error(TNBP_EINVAL, "NULL program or observable");
+    auto r = std::make_unique<tnbp::Request>();
+    r->source = tnbp::Request::QASM;
+    r->chi = chi; r->tol = bp_tol; r->maxit = bp_max_iter; r->sv_min = sv_min;
+    char opts[64];
+    std::snprintf(opts, sizeof(opts), "qasm opt=%d eps=%a\n", do_opt_tpo ? 1 : 0, do_opt_tpo ? eps_opt_tpo : 0.0);
+    r->tpos = srv->s->tpo_set(std::string(opts) + qasm_src,
+                              [&](tnbp_host::Edges& e, std::vector<tnbp_host::Layer>& layers) {
+                                const auto prog = tnbp_host::parse_qasm(qasm_src);
+                                e = tnbp_host::qasm_edges(prog);
+                                layers = tnbp_host::qasm_tpo(prog, e);
+                                if (do_opt_tpo)
+                                  for (auto& l : layers) tnbp_host::opt_tpo_svd(e, l, eps_opt_tpo);
+                              });
+    r->steps = (int)r->tpos->layers.size();
+    // the estimator app's observable: load_sparse_pauli_op + ClassifyOps
+    int64_t dropped = 0;
+    const auto terms = tnbp_host::pauli_terms(pauli_text, r->tpos->edges, &dropped);
+    const auto labels = tnbp_host::site_labels(r->tpos->edges);
+    for (const auto& t : terms) {
+      if (t.kind == 1 && !std::binary_search(labels.begin(), labels.end(), t.q0))
+        throw tnbp::Error(TNBP_EINVAL, "one-site term on qubit " + std::to_string(t.q0) + " that no two-qubit gate touches");
+      r->kind.push_back(t.kind);
+      r->q0.push_back(t.q0);
+      r->q1.push_back(t.q1);
+      r->letters.push_back(t.l0);
+      r->letters.push_back(t.kind == 2 ? t.l1 : 'I');
+      r->coeff.push_back(t.coeff_re);
+      r->coeff.push_back(t.coeff_im);
+    }
+    const int64_t id = srv->s->submit(std::move(r));
+    if (request_id) *request_id = id;
+  });
+}
+
+int tnbp_server_tpo_cache_stats(tnbp_server* srv, int64_t* hits, int64_t* misses, int64_t* entries) {
+  return sguard([&] {
+    if (!srv) throw tnbp::Error(TNBP_EINVAL, "server is NULL");
+    if (hits) *hits = srv->s->cache_hits;
+    if (misses) *misses = srv->s->cache_misses;
+    if (entries) *entries = (int64_t)srv->s->tpo_cache.size();
   });
 }
 

@@ -4,17 +4,33 @@
 
 #include <cstdint>
 #include <deque>
+#include <functional>
+#include <list>
 #include <map>
 #include <memory>
 #include <string>
 #include <vector>
 
 #include "engine.h"
+#include "host_setup.h"
 
 namespace tnbp {
 
+// Device TPO layers of one circuit on one edge list, read-only and shared
+// by every request built from the same circuit.
+struct TpoSet {
+  std::vector<std::pair<int, int>> edges;
+  std::vector<std::unique_ptr<Tpo>> layers;
+  std::vector<int> rank_max;  // per edge: largest TPO bond dimension of any layer
+  uint64_t device_bytes = 0;
+};
+
 struct Request {
   enum Phase { QUEUED, ABSORB, BP, TRUNC, MEASURE, DONE };
+  // KICKED_ISING: the one layer of tpos applied `steps` times; QASM: the
+  // layers of tpos in order (steps = their number)
+  enum Source { KICKED_ISING, QASM };
+  Source source = KICKED_ISING;
   int64_t id = 0;
   int L = 0, chi = 0, steps = 0, maxit = 0;
   double theta_j = 0, theta_h = 0, tol = 0, sv_min = 0;
@@ -23,7 +39,7 @@ struct Request {
   std::vector<double> coeff;
   Phase phase = QUEUED;
   std::unique_ptr<Job> job;
-  std::unique_ptr<Tpo> tpo;
+  std::shared_ptr<const TpoSet> tpos;
   int step = 0, bp_iters = 0;
   double prev_cond = 0;
   uint64_t footprint = 0;
@@ -45,10 +61,19 @@ struct Server {
   std::vector<int64_t> active;
   uint64_t in_use = 0;
   SweepBatch batch;
+  // TPO cache keyed by the circuit (and its TPO options), least recently
+  // used evicted first; requests keep their set alive after eviction
+  std::map<std::string, std::shared_ptr<const TpoSet>> tpo_cache;
+  std::list<std::string> tpo_lru;
+  size_t tpo_cache_cap = 32;
+  int64_t cache_hits = 0, cache_misses = 0;
 
   Server(int precision, uint64_t budget_bytes, int max_active_jobs);
   ~Server();
   int64_t submit(std::unique_ptr<Request> r);
+  std::shared_ptr<const TpoSet> tpo_set(const std::string& key,
+                                        const std::function<void(tnbp_host::Edges&,
+                                                                 std::vector<tnbp_host::Layer>&)>& build);
   void step(int* n_active, int* n_queued, int* n_done);
   uint64_t footprint(const Request& r) const;
   void start(Request& r);
