@@ -269,6 +269,33 @@ int tnbp_measure_pauli_sum(tnbp_job* job, int64_t n_terms, const int32_t* kind,
                            const int32_t* q0, const int32_t* q1, const char* letters,
                            const double* coeff, double* per_term_out, double* sum_out);
 
+/* Pauli products on any distinct qubits, including those ClassifyOps drops
+   (include/tnbp/parser/paulitotpo.h:111-132: non-adjacent pairs, three or
+   more qubits), which the reference does not measure.  Each term is
+   measured on a tree cluster: the union of the shortest paths
+   (FindShortestPath, graph.h:57-108) from its first qubit to the others,
+   contracted exactly with its ket and bra layers, the Pauli letters on the
+   qubit sites and the BP messages on every leg leaving the tree;
+   <P> = Z(P) / Z(identity).  Exact where the graph is a tree (BP messages are
+   exact environments there); for an adjacent pair it equals the two-site
+   measurement.  n_qubits[t] >= 2; qubits and letters hold the terms one
+   after another; values_out (2 doubles per term) and sum_out may be NULL. */
+int tnbp_measure_cluster(tnbp_job* job, int64_t n_terms, const int32_t* n_qubits,
+                         const int32_t* qubits, const char* letters, const double* coeff,
+                         double* values_out, double* sum_out);
+
+/* Every row of a sparse-Pauli text (load_sparse_pauli_op,
+   include/pauli/sparse_pauli.h:52-97): kinds_out[row] = 0 identity, 1 one
+   qubit, 2 adjacent pair (the two kinds ClassifyOps keeps; measured as
+   tnbp_measure_pauli_sum does), 3 any other product.  With clusters == 0,
+   kind-3 rows are not measured (NaN), as the reference drops them, and
+   sum_out = sum over kinds 1 and 2; with clusters != 0 they are measured by
+   tnbp_measure_cluster and sum_out adds them and the identity rows (value 1).
+   values_out: 2 doubles per row.  Call with cap_rows 0 to size. */
+int tnbp_measure_pauli_text(tnbp_job* job, const char* text, int32_t clusters, double* values_out,
+                            int32_t* kinds_out, int64_t cap_rows, int64_t* n_rows_out,
+                            double* sum_out);
+
 /* Time spent in the job's last bp sweep kernels (ms, CUDA events) and the
    algorithmic flops/bytes of one sweep at the current shapes. */
 int tnbp_sweep_stats(const tnbp_job* job, double* last_sweep_ms, double* flops,

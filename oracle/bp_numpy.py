@@ -292,6 +292,87 @@ def measure_2site(edges, V, E, pair, O):
     return num / den
 
 
+def shortest_path(edges, src, dst):
+    """FindShortestPath (include/tnbp/framework/graph.h:57-108): BFS from src,
+    neighbours in edge-list order, stopping when dst is dequeued."""
+    adj = {s: [] for s in sites_of(edges)}
+    for a, b in edges:
+        adj[a].append(b)
+        adj[b].append(a)
+    if src not in adj or dst not in adj:
+        return []
+    prev = {src: None}
+    queue = [src]
+    head = 0
+    while head < len(queue):
+        u = queue[head]
+        head += 1
+        if u == dst:
+            break
+        for v in adj[u]:
+            if v not in prev:
+                prev[v] = u
+                queue.append(v)
+    if dst not in prev:
+        return []
+    path = [dst]
+    while prev[path[-1]] is not None:
+        path.append(prev[path[-1]])
+    return path[::-1]
+
+
+def cluster_tree(edges, qubits):
+    """The tree cluster of a Pauli product on `qubits`: the union of the
+    shortest paths from qubits[0] to each other qubit, as {site: parent}
+    (the first qubit's parent is None)."""
+    parent = {qubits[0]: None}
+    for q in qubits[1:]:
+        path = shortest_path(edges, qubits[0], q)
+        for u, v in zip(path, path[1:]):
+            assert parent.get(v, u) == u, "paths from the first qubit do not form a tree"
+            parent[v] = u
+    return parent
+
+
+def measure_cluster(edges, V, E, qubits, letters):
+    """A Pauli product on distinct qubits measured on its tree cluster (the
+    terms ClassifyOps drops; not in the reference).  The ket and bra layers of
+    the tree's sites, the Pauli letters on the qubit sites (identity
+    elsewhere) and the BP messages on every leg leaving the tree are
+    contracted exactly: Z(P) / Z(identity).  Each site is first reduced to a
+    tensor over its tree legs (ket legs, then bra legs), then the tree is one
+    einsum."""
+    sites = sites_of(edges)
+    parent = cluster_tree(edges, list(qubits))
+    tree_edges = set()
+    for v, u in parent.items():
+        if u is not None:
+            tree_edges.add([m for m, e in enumerate(edges) if e in ((u, v), (v, u))][0])
+    opmap = dict(zip(qubits, letters))
+    te = sorted(tree_edges)
+    letter_of = {m: (2 * i, 2 * i + 1) for i, m in enumerate(te)}  # (ket, bra) einsum ids
+
+    def z(with_ops):
+        args = []
+        for s in parent:
+            v = V[sites.index(s)]
+            g = v.ndim - 1
+            bonds = bonds_of(edges, s)
+            W = v.copy()
+            for k, m in enumerate(bonds):
+                if m not in tree_edges:
+                    W = _absorb_leg(W, k, E[in_msg(edges, s, m)])
+            O = pauli_op(opmap[s]) if (with_ops and s in opmap) else np.eye(2, dtype=np.complex128)
+            W = np.tensordot(W, O, axes=([g], [0]))
+            closed = [k for k, m in enumerate(bonds) if m not in tree_edges] + [g]
+            T = np.tensordot(W, v.conj(), axes=(closed, closed))
+            open_m = [m for m in bonds if m in tree_edges]
+            args += [T, [letter_of[m][0] for m in open_m] + [letter_of[m][1] for m in open_m]]
+        return np.einsum(*args, [])
+
+    return z(True) / z(False)
+
+
 # --------------------------------------------------------------- Pauli
 PAULI = {
     "I": [1, 0, 0, 1],

@@ -72,3 +72,32 @@ def test_estimator_app_with_opt_tpo(precision, tol):
     assert len(one) == len(ref["one"]) and len(two) == len(ref["two"]), out
     for a, b in zip(one + two, ref["one"] + ref["two"]):
         assert abs(a - b) <= tol, (a, b)
+
+
+def test_estimator_app_measures_cluster_terms():
+    """--measure_clusters: the rows the reference drops, measured on their
+    tree clusters.  On the chain (a tree, no truncation) they are exact; the
+    oracle's cluster contraction of the reference's own final state gives
+    the same values (a gauge-invariant quantity, 1e-9)."""
+    import numpy as np
+
+    import bp_numpy as bn
+    R, meta = load_probe(os.path.join(HERE, "golden", "probe_chain6.npz"))
+    one, two, out = _run("chain6", meta, "c128", ("--measure_clusters",))
+    rows = re.findall(r"Expectation value of cluster operator in row (\d+) (\S+)", out)
+    assert rows, out
+    pauli = open(os.path.join(HERE, "golden", "inputs", "chain6.txt")).read()
+    ed = R["edges"].real.astype(int)
+    edges = [(int(ed[0, i]), int(ed[1, i])) for i in range(ed.shape[1])]
+    t = int(R["n_layers"].real) - 1
+    V = [R[f"step/{t}/trunc/V/{s}"] for s in range(len(bn.sites_of(edges)))]
+    E = [R[f"step/{t}/trunc/E/{m}"] for m in range(2 * len(edges))]
+    lines = [l.strip() for l in pauli.splitlines()]
+    lines = [l for l in lines if l and not l.startswith("#") and not l.startswith("//")]
+    for r, v in rows:
+        ps = lines[int(r)].split()[-1].upper()
+        qs = [i for i in range(len(ps)) if ps[len(ps) - 1 - i] != "I"]
+        ls = [ps[len(ps) - 1 - q] for q in qs]
+        want = bn.measure_cluster(edges, V, E, qs, ls)
+        assert abs(float(v) - want.real) <= 1e-9, (r, v, want)
+    assert "Sum of c_k <P_k> over all terms" in out

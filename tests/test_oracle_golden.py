@@ -119,3 +119,43 @@ def test_chain_is_exact_against_statevector():
     ref = bn.statevector_expect(n, gates, terms)
     _, vals = bn.pauli_sum(edges, V, E, terms)
     np.testing.assert_allclose(np.array(vals), np.array(ref), atol=1e-10)
+    # products ClassifyOps drops, on their tree clusters: exact on a chain
+    cl = [((0, 3), ("X", "Z")), ((4, 1), ("Y", "X")), ((1, 2, 4), ("Z", "Y", "X")),
+          ((5, 0, 2, 3), ("X", "Z", "Y", "Z")), ((3, 5), ("Z", "Z"))]
+    ref = bn.statevector_expect(n, gates, [(3, q, l, 1.0) for q, l in cl])
+    got = [bn.measure_cluster(edges, V, E, q, l) for q, l in cl]
+    np.testing.assert_allclose(np.array(got), np.array(ref), atol=1e-10)
+
+
+@pytest.mark.parametrize("path", PROBES, ids=[os.path.basename(p) for p in PROBES])
+def test_cluster_of_an_adjacent_pair_is_the_two_site_measurement(path):
+    """The tree cluster of an adjacent pair is the pair itself: the cluster
+    contraction equals measure.h's two-site value on the reference's final
+    (loopy-BP) state."""
+    R, meta = load_probe(path)
+    edges = _edges(R)
+    ns, ne = len(bn.sites_of(edges)), len(edges)
+    t = int(R["n_layers"].real) - 1
+    V = [R[f"step/{t}/trunc/V/{s}"] for s in range(ns)]
+    E = [R[f"step/{t}/trunc/E/{m}"] for m in range(2 * ne)]
+    for (a, b) in edges:
+        for la, lb in (("X", "Z"), ("Y", "Y"), ("Z", "X")):
+            v2 = bn.measure_2site(edges, V, E, (a, b), bn.pauli_two(la, lb))
+            vc = bn.measure_cluster(edges, V, E, (b, a), (lb, la))
+            assert abs(v2 - vc) < 1e-12
+
+
+def test_oracle_shortest_paths_are_the_reference_paths():
+    """FindShortestPath restated in the oracle against the reference's own
+    paths (oracle/ref_hostparity.cc fixtures)."""
+    import json
+    n = 0
+    for p in sorted(glob.glob(os.path.join(HERE, "golden", "host_*.json"))):
+        H = json.load(open(p))
+        if "paths" not in H:
+            continue
+        edges = [tuple(e) for e in H["edges"]]
+        for src, dst, path in H["paths"]:
+            assert bn.shortest_path(edges, src, dst) == path
+            n += 1
+    assert n > 50

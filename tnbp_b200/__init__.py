@@ -82,6 +82,8 @@ _SIGS = {
     "tnbp_measure_1site": [_vp, C.c_int64, _i64p, _f64p, _f64p],
     "tnbp_measure_2site": [_vp, C.c_int64, _i32p, _f64p, _f64p],
     "tnbp_measure_pauli_sum": [_vp, C.c_int64, _i32p, _i32p, _i32p, C.c_char_p, _f64p, _f64p, _f64p],
+    "tnbp_measure_cluster": [_vp, C.c_int64, _i32p, _i32p, C.c_char_p, _f64p, _f64p, _f64p],
+    "tnbp_measure_pauli_text": [_vp, C.c_char_p, C.c_int32, _f64p, _i32p, C.c_int64, _i64p, _f64p],
     "tnbp_sweep_stats": [_vp, _f64p, _f64p, _f64p],
     "tnbp_sweep_totals": [_vp, _f64p, _f64p, _f64p, _i64p],
     "tnbp_server_create": [C.c_int32, C.c_uint64, C.c_int32, C.POINTER(_vp)],
@@ -542,6 +544,38 @@ def Measure(state, where, ops):
         _chk(lib.tnbp_measure_2site(state.h, len(where), _p(pr, _i32p), _p(o.view(np.float64), _f64p),
                                     _p(out.view(np.float64), _f64p)))
     return out
+
+
+def MeasureCluster(state, terms, coeffs=None):
+    """Pauli products on any distinct qubits, each measured on its tree
+    cluster (tnbp_measure_cluster).  terms: list of (qubits, letters);
+    returns (values per term, sum_k c_k <P_k>)."""
+    n = len(terms)
+    if n == 0:
+        return np.zeros(0, np.complex128), 0j
+    nq = np.array([len(q) for q, _ in terms], np.int32)
+    qs = np.ascontiguousarray(np.concatenate([np.asarray(q, np.int32) for q, _ in terms]))
+    letters = "".join(l for _, l in terms).encode()
+    co = np.ones(n, np.complex128) if coeffs is None else np.ascontiguousarray(coeffs, np.complex128)
+    vals = np.zeros(n, np.complex128)
+    tot = np.zeros(1, np.complex128)
+    _chk(lib.tnbp_measure_cluster(state.h, n, _p(nq, _i32p), _p(qs, _i32p), letters, _p(co.view(np.float64), _f64p),
+                                  _p(vals.view(np.float64), _f64p), _p(tot.view(np.float64), _f64p)))
+    return vals, complex(tot[0])
+
+
+def MeasurePauliText(state, text, clusters=True):
+    """Every row of a sparse-Pauli text (tnbp_measure_pauli_text): returns
+    (sum, values per row, kinds per row)."""
+    n = C.c_int64()
+    s = text.encode()
+    _chk(lib.tnbp_measure_pauli_text(state.h, s, 1 if clusters else 0, None, None, 0, C.byref(n), None))
+    vals = np.zeros(max(1, n.value), np.complex128)
+    kinds = np.zeros(max(1, n.value), np.int32)
+    tot = np.zeros(1, np.complex128)
+    _chk(lib.tnbp_measure_pauli_text(state.h, s, 1 if clusters else 0, _p(vals.view(np.float64), _f64p),
+                                     _p(kinds, _i32p), n.value, C.byref(n), _p(tot.view(np.float64), _f64p)))
+    return complex(tot[0]), vals[: n.value], kinds[: n.value]
 
 
 class Server:

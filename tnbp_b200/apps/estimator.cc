@@ -7,8 +7,11 @@
 //   --max_bp_iterations N  --sv_min X  --truncation_error X (accepted, unused
 //   by the reference too)  --backend default  --do_opt_tpo N (nonzero:
 //   OptTPObySVD on every layer)  --eps_opt_tpo X
-// plus --precision c128|mixed|c64 (default c128, the drop-in) and --sum
-// (print sum_k c_k <P_k>, which the reference does not compute).
+// plus --precision c128|mixed|c64 (default c128, the drop-in), --sum
+// (print sum_k c_k <P_k>, which the reference does not compute) and
+// --measure_clusters (also measure the terms the reference drops --
+// non-adjacent pairs, three or more qubits -- on their tree clusters, and
+// print them with their file row).
 // Printed lines follow the reference's wording for the per-layer BP
 // condition, the per-edge truncation results and the per-term expectation
 // values (one-site terms first, then two-site terms, each in file order);
@@ -49,6 +52,7 @@ struct Options {
   double eps_opt_tpo = 1.0e-8;
   int precision = TNBP_C128;
   bool print_sum = false;
+  bool clusters = false;
 };
 
 Options parse(int argc, char** argv) {
@@ -68,6 +72,7 @@ Options parse(int argc, char** argv) {
     else if (a == "--sv_min") o.sv_min = std::atof(next().c_str());
     else if (a == "--truncation_error") o.truncation_error = std::atof(next().c_str());
     else if (a == "--sum") o.print_sum = true;
+    else if (a == "--measure_clusters") o.clusters = true;
     else if (a == "--do_opt_tpo") o.do_opt_tpo = std::atoi(next().c_str()) != 0;
     else if (a == "--eps_opt_tpo") o.eps_opt_tpo = std::atof(next().c_str());
     else if (a == "--precision") {
@@ -184,6 +189,19 @@ int run(const Options& o) {
       std::cout << " Expectation value of two site operator at sites (" << q0[k] << "," << q1[k] << ") "
                 << per[2 * k] << "\n";
   if (o.print_sum) std::cout << " Sum of c_k <P_k> = " << sum[0] << " " << sum[1] << "\n";
+  if (o.clusters) {
+    int64_t nrows = 0;
+    check(tnbp_measure_pauli_text(job, pauli.c_str(), 1, nullptr, nullptr, 0, &nrows, nullptr),
+          "tnbp_measure_pauli_text");
+    std::vector<double> vals(2 * nrows + 2), all(2);
+    std::vector<int32_t> kinds(nrows + 1);
+    check(tnbp_measure_pauli_text(job, pauli.c_str(), 1, vals.data(), kinds.data(), nrows, &nrows, all.data()),
+          "tnbp_measure_pauli_text");
+    for (int64_t r = 0; r < nrows; ++r)
+      if (kinds[r] == 3)
+        std::cout << " Expectation value of cluster operator in row " << r << " " << vals[2 * r] << "\n";
+    if (o.print_sum) std::cout << " Sum of c_k <P_k> over all terms = " << all[0] << " " << all[1] << "\n";
+  }
   check(tnbp_job_destroy(job), "tnbp_job_destroy");
   return 0;
 }

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -547,45 +548,123 @@ int tnbp_measure_2site(tnbp_job* job, int64_t n, const int32_t* pairs, const dou
   });
 }
 
+}  // extern "C"
+
+namespace {
+// One kept term of ClassifyOps as the device measurement takes it.
+tnbp::TermSpec term_spec(const tnbp::Job& J, int kind, int q0, int q1, char l0, char l1, double cre, double cim) {
+  tnbp::TermSpec t;
+  std::memset(&t, 0, sizeof(t));
+  t.kind = kind;
+  t.coeff[0] = cre;
+  t.coeff[1] = cim;
+  if (kind == 1) {
+    auto it = J.g.index_of.find(q0);
+    need(it != J.g.index_of.end(), "one-site term on a qubit outside the lattice");
+    t.site_a = it->second;
+    auto P = tnbp_host::pauli_list(l0);
+    for (int k = 0; k < 4; ++k) { t.op[2 * k] = P[k].real(); t.op[2 * k + 1] = P[k].imag(); }
+  } else if (kind == 2) {
+    t.edge = J.edge_of(q0, q1);
+    need(t.edge >= 0, "two-site term on a non-adjacent pair");
+    t.label_a = q0;
+    auto Pa = tnbp_host::pauli_list(l0);
+    auto Pb = tnbp_host::pauli_list(l1);
+    // O[i0, i1, i2, i3] = Pa[i0, i2] Pb[i1, i3]  (paulitotpo.h:73-91)
+    for (int i0 = 0; i0 < 2; ++i0)
+      for (int i1 = 0; i1 < 2; ++i1)
+        for (int i2 = 0; i2 < 2; ++i2)
+          for (int i3 = 0; i3 < 2; ++i3) {
+            const auto v = Pa[i0 + 2 * i2] * Pb[i1 + 2 * i3];
+            const int idx = i0 + 2 * i1 + 4 * i2 + 8 * i3;
+            t.op[2 * idx] = v.real();
+            t.op[2 * idx + 1] = v.imag();
+          }
+  } else {
+    throw Error(TNBP_EINVAL, "term kind must be 1 or 2");
+  }
+  return t;
+}
+}  // namespace
+
+extern "C" {
+
 int tnbp_measure_pauli_sum(tnbp_job* job, int64_t n, const int32_t* kind, const int32_t* q0, const int32_t* q1,
                            const char* letters, const double* coeff, double* per_term, double* sum) {
   return guard([&] {
     need(job && (n == 0 || (kind && q0 && q1 && letters && coeff)), "NULL argument");
     auto& J = *job->j;
-    std::vector<tnbp::TermSpec> terms(n);
+    std::vector<tnbp::TermSpec> terms;
+    for (int64_t i = 0; i < n; ++i)
+      terms.push_back(term_spec(J, kind[i], q0[i], q1[i], letters[2 * i], letters[2 * i + 1], coeff[2 * i],
+                                coeff[2 * i + 1]));
+    J.measure_terms(terms, per_term, sum);
+  });
+}
+
+int tnbp_measure_cluster(tnbp_job* job, int64_t n, const int32_t* n_qubits, const int32_t* qubits,
+                         const char* letters, const double* coeff, double* values, double* sum) {
+  return guard([&] {
+    need(job && (n == 0 || (n_qubits && qubits && letters && coeff)), "NULL argument");
+    std::vector<tnbp::ClusterTerm> terms(n);
+    int64_t o = 0;
     for (int64_t i = 0; i < n; ++i) {
-      auto& t = terms[i];
-      std::memset(&t, 0, sizeof(t));
-      t.kind = kind[i];
-      t.coeff[0] = coeff[2 * i];
-      t.coeff[1] = coeff[2 * i + 1];
-      if (t.kind == 1) {
-        auto it = J.g.index_of.find(q0[i]);
-        need(it != J.g.index_of.end(), "one-site term on a qubit outside the lattice");
-        t.site_a = it->second;
-        auto P = tnbp_host::pauli_list(letters[2 * i]);
-        for (int k = 0; k < 4; ++k) { t.op[2 * k] = P[k].real(); t.op[2 * k + 1] = P[k].imag(); }
-      } else if (t.kind == 2) {
-        t.edge = J.edge_of(q0[i], q1[i]);
-        need(t.edge >= 0, "two-site term on a non-adjacent pair");
-        t.label_a = q0[i];
-        auto Pa = tnbp_host::pauli_list(letters[2 * i]);
-        auto Pb = tnbp_host::pauli_list(letters[2 * i + 1]);
-        // O[i0, i1, i2, i3] = Pa[i0, i2] Pb[i1, i3]  (paulitotpo.h:73-91)
-        for (int i0 = 0; i0 < 2; ++i0)
-          for (int i1 = 0; i1 < 2; ++i1)
-            for (int i2 = 0; i2 < 2; ++i2)
-              for (int i3 = 0; i3 < 2; ++i3) {
-                const auto v = Pa[i0 + 2 * i2] * Pb[i1 + 2 * i3];
-                const int idx = i0 + 2 * i1 + 4 * i2 + 8 * i3;
-                t.op[2 * idx] = v.real();
-                t.op[2 * idx + 1] = v.imag();
-              }
-      } else {
-        throw Error(TNBP_EINVAL, "term kind must be 1 or 2");
+      need(n_qubits[i] >= 2 && n_qubits[i] <= 64, "a cluster term has 2 to 64 qubits");
+      terms[i].labels.assign(qubits + o, qubits + o + n_qubits[i]);
+      for (int k = 0; k < n_qubits[i]; ++k) terms[i].letters.push_back((char)std::toupper((unsigned char)letters[o + k]));
+      terms[i].coeff[0] = coeff[2 * i];
+      terms[i].coeff[1] = coeff[2 * i + 1];
+      o += n_qubits[i];
+    }
+    job->j->measure_clusters(terms, values, sum);
+  });
+}
+
+int tnbp_measure_pauli_text(tnbp_job* job, const char* text, int32_t clusters, double* values, int32_t* kinds,
+                            int64_t cap, int64_t* n_rows, double* sum) {
+  return guard([&] {
+    need(job && text, "NULL argument");
+    auto& J = *job->j;
+    const auto rows = tnbp_host::pauli_strings(text, J.g.edges);
+    const int64_t n = (int64_t)rows.size();
+    if (n_rows) *n_rows = n;
+    if (!values && !kinds && !sum) return;  // sizing call
+    need(!(values || kinds) || cap >= n, "output capacity too small");
+    std::vector<tnbp::TermSpec> kept;
+    std::vector<int64_t> kept_row;
+    std::vector<tnbp::ClusterTerm> cl;
+    std::vector<int64_t> cl_row;
+    std::vector<double> out(2 * std::max<int64_t>(n, 1), std::nan(""));
+    double sr = 0.0, si = 0.0;  // identity terms
+    for (int64_t r = 0; r < n; ++r) {
+      const auto& t = rows[r];
+      if (kinds) kinds[r] = t.kind;
+      if (t.kind == 0) {
+        out[2 * r] = 1.0;
+        out[2 * r + 1] = 0.0;
+        if (clusters) { sr += t.coeff_re; si += t.coeff_im; }
+      } else if (t.kind == 1 || t.kind == 2) {
+        kept.push_back(term_spec(J, t.kind, t.qubits[0], t.kind == 2 ? t.qubits[1] : -1, t.letters[0],
+                                 t.kind == 2 ? t.letters[1] : 'I', t.coeff_re, t.coeff_im));
+        kept_row.push_back(r);
+      } else if (clusters) {
+        tnbp::ClusterTerm c;
+        c.labels = t.qubits;
+        c.letters.assign(t.letters.begin(), t.letters.end());
+        c.coeff[0] = t.coeff_re;
+        c.coeff[1] = t.coeff_im;
+        cl.push_back(c);
+        cl_row.push_back(r);
       }
     }
-    J.measure_terms(terms, per_term, sum);
+    std::vector<double> kv(2 * std::max<size_t>(kept.size(), 1)), cv(2 * std::max<size_t>(cl.size(), 1));
+    double ks[2] = {0.0, 0.0}, cs[2] = {0.0, 0.0};
+    if (!kept.empty()) J.measure_terms(kept, kv.data(), ks);
+    if (!cl.empty()) J.measure_clusters(cl, cv.data(), cs);
+    for (size_t k = 0; k < kept.size(); ++k) { out[2 * kept_row[k]] = kv[2 * k]; out[2 * kept_row[k] + 1] = kv[2 * k + 1]; }
+    for (size_t k = 0; k < cl.size(); ++k) { out[2 * cl_row[k]] = cv[2 * k]; out[2 * cl_row[k] + 1] = cv[2 * k + 1]; }
+    if (values) std::memcpy(values, out.data(), 2 * n * sizeof(double));
+    if (sum) { sum[0] = ks[0] + cs[0] + sr; sum[1] = ks[1] + cs[1] + si; }
   });
 }
 

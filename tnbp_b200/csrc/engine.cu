@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <complex>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -21,6 +22,7 @@
 
 #include "../../include/tnbp_b200.h"
 #include "engine.h"
+#include "host_setup.h"
 #include "kernels.cuh"
 #include "measure.cuh"
 #include "tc_leg.cuh"
@@ -1209,18 +1211,16 @@ void Job::normalize_sites() {
 }
 
 // -------------------------------------------------------------- measurement
-// Reduced density matrices: one-site rho over the physical leg
-// (measure.h:46-89), two-site environments over (target leg, physical leg)
-// (measure.h:168-245).  Returns device buffers holding FP64 matrices.
-void Job::compute_envs(const std::vector<int>& sites1, const std::vector<std::pair<int, int>>& sidelegs,
-                       DevBuf& out1, DevBuf& out2, std::vector<size_t>& off2) {
-  const int ne = (int)g.edges.size();
-  (void)ne;
-  // W = V x (incoming messages on the selected legs)
-  struct Req { int site; int keep_leg; };  // keep_leg = -1: absorb all legs
-  std::vector<Req> reqs;
-  for (int s : sites1) reqs.push_back({s, -1});
-  for (auto& p : sidelegs) reqs.push_back({p.first, p.second});
+// Environments of single sites as FP64 Gram matrices: for request r,
+//   W = V_site with a matrix absorbed on every leg except keep_leg (the
+//       incoming BP message, or r.mats[k] when that is set: a D x D matrix in
+//       storage precision applied as W[..j..] = sum_i V[..i..] M[i, j]),
+//   env[(t + D p), (t' + D p')] = sum_x W[x, t, p] conj(V[x, t', p'])
+// over the kept leg t (D = its dimension) and the physical leg p; with
+// keep_leg = -1 every bond leg is absorbed and env is the d x d one-site
+// rho.  Outputs are packed in request order; off[i] is request i's offset
+// (double2 elements).
+void Job::env_grams(const std::vector<EnvReq>& reqs, DevBuf& out, std::vector<size_t>& off) {
   std::vector<size_t> woff(reqs.size());
   size_t wtot = 0;
   for (size_t i = 0; i < reqs.size(); ++i) { woff[i] = wtot; wtot += align_elems(site_elems(reqs[i].site)); }
@@ -1236,8 +1236,9 @@ void Job::compute_envs(const std::vector<int>& sites1, const std::vector<std::pa
     const auto sh = site_shape(c.site);
     for (size_t k = 0; k < g.legs[c.site].size(); ++k) {
       if ((int)k == reqs[i].keep_leg) continue;
+      const void* m = k < reqs[i].mats.size() ? reqs[i].mats[k] : nullptr;
       c.legs.push_back((int)k);
-      c.mats.push_back(mptr(cur, g.in_msg(c.site, (int)k)));
+      c.mats.push_back(m ? m : mptr(cur, g.in_msg(c.site, (int)k)));
       c.dout.push_back(sh[k]);
     }
     if (c.legs.empty()) copy_only.push_back(i);
@@ -1252,10 +1253,9 @@ void Job::compute_envs(const std::vector<int>& sites1, const std::vector<std::pa
   std::vector<long long> gb;
   std::vector<PartialSumTask> pt;
   long long nb = 0;
-  size_t ptot = 0, o1 = 0, o2 = 0;
+  size_t ptot = 0, otot = 0;
   std::vector<size_t> poff;
-  std::vector<size_t> ooff;
-  off2.clear();
+  off.clear();
   for (size_t i = 0; i < reqs.size(); ++i) {
     const int s = reqs[i].site;
     const auto sh = site_shape(s);
@@ -1285,21 +1285,20 @@ void Job::compute_envs(const std::vector<int>& sites1, const std::vector<std::pa
     nb += (long long)t.nchunk * t.ctiles * t.ctiles;
     poff.push_back(ptot);
     ptot += (size_t)t.nchunk * t.C * t.C;
-    if (reqs[i].keep_leg < 0) { ooff.push_back(o1); o1 += (size_t)t.C * t.C; }
-    else { ooff.push_back(o2); off2.push_back(o2); o2 += (size_t)t.C * t.C; }
+    off.push_back(otot);
+    otot += (size_t)t.C * t.C;
     gt.push_back(t);
   }
   DevBuf part;
   part.alloc(std::max<size_t>(ptot, 1) * sizeof(double2), stream);
-  out1.alloc(std::max<size_t>(o1, 1) * sizeof(double2), stream);
-  out2.alloc(std::max<size_t>(o2, 1) * sizeof(double2), stream);
+  out.alloc(std::max<size_t>(otot, 1) * sizeof(double2), stream);
   for (size_t i = 0; i < gt.size(); ++i) {
     gt[i].partial = static_cast<double2*>(part.p) + poff[i];
     PartialSumTask p;
     p.partial = gt[i].partial;
     p.nchunk = gt[i].nchunk;
     p.n = gt[i].C * gt[i].C;
-    p.out = static_cast<double2*>(reqs[i].keep_leg < 0 ? out1.p : out2.p) + ooff[i];
+    p.out = static_cast<double2*>(out.p) + off[i];
     pt.push_back(p);
   }
   DevBuf dgt, dgb, dpt;
@@ -1314,6 +1313,19 @@ void Job::compute_envs(const std::vector<int>& sites1, const std::vector<std::pa
     CK(cudaGetLastError());
   }
   CK(cudaStreamSynchronize(stream));
+}
+
+// Reduced density matrices: one-site rho over the physical leg
+// (measure.h:46-89), two-site environments over (target leg, physical leg)
+// (measure.h:168-245).  Returns device buffers holding FP64 matrices.
+void Job::compute_envs(const std::vector<int>& sites1, const std::vector<std::pair<int, int>>& sidelegs,
+                       DevBuf& out1, DevBuf& out2, std::vector<size_t>& off2) {
+  std::vector<EnvReq> r1, r2;
+  for (int s : sites1) r1.push_back({s, -1, {}});
+  for (auto& p : sidelegs) r2.push_back({p.first, p.second, {}});
+  std::vector<size_t> off1;
+  env_grams(r1, out1, off1);
+  env_grams(r2, out2, off2);
 }
 
 void Job::measure_terms(const std::vector<TermSpec>& terms, double* values, double* sum) {
@@ -1384,6 +1396,189 @@ void Job::measure_terms(const std::vector<TermSpec>& terms, double* values, doub
   CK(cudaStreamSynchronize(stream));
   if (values) std::memcpy(values, hv.data(), terms.size() * 2 * sizeof(double));
   if (sum) { sum[0] = hs[0]; sum[1] = hs[1]; }
+}
+
+// Pauli products on any set of distinct sites -- the terms ClassifyOps drops
+// (paulitotpo.h:111-132: pairs that are not adjacent, three or more qubits)
+// -- measured on a tree cluster T: the union of the shortest paths
+// (FindShortestPath, graph.h:57-108) from the first qubit's site to every
+// other qubit's site.  T's ket and bra layers, the term's Pauli on its qubit
+// sites and the incoming BP messages on every leg that leaves T are
+// contracted leaf to root: a tree site absorbs its children's results on
+// their legs (as BP messages are absorbed) and BP messages on its other
+// legs; its Gram environment over (leg toward its parent, physical leg)
+// contracted with its one-site operator is its result X[t, t'].  At the root,
+// its environment toward its first child, contracted with its operator,
+// meets that child's result: Z = sum_{t,t'} X_child[t,t'] X_root[t,t'], the
+// pairing of the two-site measurement (measure.h:255-294).  The value is
+// Z(P) / Z(identity).  On a tree graph BP messages are exact environments,
+// so the value is exact there; for an adjacent pair it is the two-site
+// measurement.  Tree levels of every term are batched into shared launches.
+void Job::measure_clusters(const std::vector<ClusterTerm>& terms, double* values, double* sum) {
+  TNBP_TRACE_SCOPE("measure.clusters");
+  struct Node {
+    int site;
+    int parent = -1;      // node index
+    int parent_leg = -1;  // leg of this site toward its parent
+    std::vector<int> children;
+    std::vector<int> child_leg;  // leg of this site toward each child
+    char letter = 'I';
+    int height = 0;
+  };
+  const auto leg_of = [&](int s, int e) {
+    const auto& L = g.legs[s];
+    return (int)(std::find(L.begin(), L.end(), e) - L.begin());
+  };
+  std::vector<std::vector<Node>> trees(terms.size());
+  int max_height = 0;
+  for (size_t i = 0; i < terms.size(); ++i) {
+    const auto& t = terms[i];
+    if (t.labels.size() < 2 || t.labels.size() != t.letters.size())
+      throw Error(TNBP_EINVAL, "a cluster term needs two or more qubits, one letter each");
+    auto& nodes = trees[i];
+    std::map<int, int> node_of;  // site -> node
+    for (size_t k = 0; k < t.labels.size(); ++k) {
+      auto it = g.index_of.find(t.labels[k]);
+      if (it == g.index_of.end())
+        throw Error(TNBP_EINVAL, "term on qubit " + std::to_string(t.labels[k]) + " outside the graph");
+      if (pd[it->second] != 2) throw Error(TNBP_EUNSUPPORTED, "cluster terms need physical dimension 2");
+      const char l = t.letters[k];
+      if (l != 'X' && l != 'Y' && l != 'Z' && l != 'I') throw Error(TNBP_EINVAL, "Pauli letters are I, X, Y, Z");
+      const auto path = tnbp_host::shortest_path(g.edges, t.labels[0], t.labels[k]);
+      if (path.empty()) throw Error(TNBP_EINVAL, "term qubits in different components of the graph");
+      int prev = -1;
+      for (size_t j = 0; j < path.size(); ++j) {
+        const int s = g.index_of.at(path[j]);
+        auto nt = node_of.find(s);
+        if (nt == node_of.end()) {
+          Node n;
+          n.site = s;
+          if (prev >= 0) {
+            const int e = edge_of(g.labels[nodes[prev].site], path[j]);
+            n.parent = prev;
+            n.parent_leg = leg_of(s, e);
+            nodes[prev].children.push_back((int)nodes.size());
+            nodes[prev].child_leg.push_back(leg_of(nodes[prev].site, e));
+          }
+          node_of[s] = (int)nodes.size();
+          nodes.push_back(n);
+          prev = (int)nodes.size() - 1;
+        } else {
+          if (prev >= 0 && nodes[nt->second].parent != prev)
+            throw Error(TNBP_EUNSUPPORTED, "shortest paths from the first qubit do not form a tree");
+          prev = nt->second;
+        }
+      }
+      Node& q = nodes[node_of.at(g.index_of.at(t.labels[k]))];
+      if (q.letter != 'I' || (k > 0 && q.site == nodes[0].site)) throw Error(TNBP_EINVAL, "repeated qubit in a term");
+      q.letter = l == 'I' ? 'i' : l;  // 'i': named identity, still a qubit of the term
+    }
+    // heights: children are created after their parents
+    for (int n = (int)nodes.size() - 1; n >= 0; --n)
+      for (int c : nodes[n].children) nodes[n].height = std::max(nodes[n].height, nodes[c].height + 1);
+    max_height = std::max(max_height, nodes[0].height);
+  }
+  // result slots: per (term, chain, node), D x D with D the dimension of the
+  // edge toward the parent (the root: toward its first child)
+  const auto slot_dim = [&](const std::vector<Node>& nodes, int n) {
+    const Node& nd = nodes[n];
+    const int leg = nd.parent >= 0 ? nd.parent_leg : nd.child_leg[0];
+    return dim[g.legs[nd.site][leg]];
+  };
+  std::vector<std::vector<size_t>> off(2 * terms.size());
+  size_t tot = 0;
+  for (size_t i = 0; i < terms.size(); ++i)
+    for (int ch = 0; ch < 2; ++ch) {
+      auto& o = off[2 * i + ch];
+      for (size_t n = 0; n < trees[i].size(); ++n) {
+        o.push_back(tot);
+        const size_t D = (size_t)slot_dim(trees[i], (int)n);
+        tot += align_elems(D * D);
+      }
+    }
+  DevBuf xs, x64, zbuf;
+  xs.alloc(std::max<size_t>(tot, 32) * esz, stream);
+  x64.alloc(std::max<size_t>(tot, 32) * sizeof(double2), stream);
+  zbuf.alloc(std::max<size_t>(2 * terms.size(), 1) * sizeof(double2), stream);
+  const auto pauli_op = [](char l, double2* op) {
+    const auto P = tnbp_host::pauli_list(l == 'i' ? 'I' : l);
+    for (int k = 0; k < 4; ++k) op[k] = make_double2(P[k].real(), P[k].imag());
+  };
+  // levels 0 .. max_height; the roots are done at their own height
+  for (int h = 0; h <= max_height; ++h) {
+    std::vector<EnvReq> reqs;
+    struct Out { size_t term; int ch; int node; };
+    std::vector<Out> outs;
+    for (size_t i = 0; i < terms.size(); ++i)
+      for (int ch = 0; ch < 2; ++ch)
+        for (size_t n = 0; n < trees[i].size(); ++n) {
+          const Node& nd = trees[i][n];
+          if (nd.height != h) continue;
+          EnvReq r;
+          r.site = nd.site;
+          const bool root = nd.parent < 0;
+          r.keep_leg = root ? nd.child_leg[0] : nd.parent_leg;
+          r.mats.assign(g.legs[nd.site].size(), nullptr);
+          for (size_t c = root ? 1 : 0; c < nd.children.size(); ++c)
+            r.mats[nd.child_leg[c]] = static_cast<char*>(xs.p) + off[2 * i + ch][nd.children[c]] * esz;
+          reqs.push_back(r);
+          outs.push_back({i, ch, (int)n});
+        }
+    if (reqs.empty()) continue;
+    DevBuf env;
+    std::vector<size_t> eoff;
+    env_grams(reqs, env, eoff);
+    std::vector<EnvOpTask> et(reqs.size());
+    for (size_t k = 0; k < reqs.size(); ++k) {
+      const Out& o = outs[k];
+      const Node& nd = trees[o.term][o.node];
+      EnvOpTask& t = et[k];
+      t.env = static_cast<const double2*>(env.p) + eoff[k];
+      t.D = slot_dim(trees[o.term], o.node);
+      t.d = 2;
+      pauli_op(o.ch == 0 ? nd.letter : 'I', t.op);
+      t.out64 = static_cast<double2*>(x64.p) + off[2 * o.term + o.ch][o.node];
+      t.out = nd.parent >= 0 ? static_cast<char*>(xs.p) + off[2 * o.term + o.ch][o.node] * esz : nullptr;
+    }
+    DevBuf det;
+    upload_vec(det, et, stream);
+    if (sprec == TNBP_C128) (k_env_op<double><<<(unsigned)et.size(), kThreads, 0, stream>>>(static_cast<EnvOpTask*>(det.p)), note_launch());
+    else (k_env_op<float><<<(unsigned)et.size(), kThreads, 0, stream>>>(static_cast<EnvOpTask*>(det.p)), note_launch());
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream));
+  }
+  // the root meets its first child
+  std::vector<PairTask> pt;
+  for (size_t i = 0; i < terms.size(); ++i)
+    for (int ch = 0; ch < 2; ++ch) {
+      const auto& nodes = trees[i];
+      const int D = slot_dim(nodes, 0);
+      PairTask p;
+      p.a = static_cast<const double2*>(x64.p) + off[2 * i + ch][nodes[0].children[0]];
+      p.b = static_cast<const double2*>(x64.p) + off[2 * i + ch][0];
+      p.n = D * D;
+      p.out = static_cast<double2*>(zbuf.p) + 2 * i + ch;
+      pt.push_back(p);
+    }
+  std::vector<double> z(4 * std::max<size_t>(terms.size(), 1), 0.0);
+  if (!pt.empty()) {
+    DevBuf dpt;
+    upload_vec(dpt, pt, stream);
+    (k_pair_dot<<<(unsigned)pt.size(), kThreads, 0, stream>>>(static_cast<PairTask*>(dpt.p)), note_launch());
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(z.data(), zbuf.p, 2 * terms.size() * sizeof(double2), cudaMemcpyDeviceToHost, stream));
+  }
+  CK(cudaStreamSynchronize(stream));
+  double sr = 0.0, si = 0.0;
+  for (size_t i = 0; i < terms.size(); ++i) {
+    const std::complex<double> zp(z[4 * i], z[4 * i + 1]), zi(z[4 * i + 2], z[4 * i + 3]);
+    const std::complex<double> v = zp / zi;
+    if (values) { values[2 * i] = v.real(); values[2 * i + 1] = v.imag(); }
+    const std::complex<double> c = std::complex<double>(terms[i].coeff[0], terms[i].coeff[1]) * v;
+    sr += c.real();
+    si += c.imag();
+  }
+  if (sum) { sum[0] = sr; sum[1] = si; }
 }
 
 int Job::edge_of(int la, int lb) const {

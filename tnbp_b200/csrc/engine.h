@@ -170,6 +170,23 @@ struct TermSpec {
 
 struct ChainEntry;
 
+// One environment request of Job::env_grams: keep_leg = -1 (one-site rho)
+// or the bond leg left open; mats[k], when given, replaces the incoming BP
+// message on leg k (a D_k x D_k matrix in storage precision).
+struct EnvReq {
+  int site;
+  int keep_leg;
+  std::vector<const void*> mats;
+};
+
+// A Pauli product on distinct sites measured on a tree cluster (see
+// Job::measure_clusters).
+struct ClusterTerm {
+  std::vector<int> labels;  // site labels of the qubits; the first is the tree root
+  std::vector<char> letters;
+  double coeff[2];
+};
+
 struct Job {
   Graph g;
   int prec;      // TNBP_C128, TNBP_C64 or TNBP_MIXED
@@ -227,6 +244,8 @@ struct Job {
   void run_chains(std::vector<ChainEntry>& chains);
   void truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_out);
   void normalize_sites();
+  void env_grams(const std::vector<EnvReq>& reqs, DevBuf& out, std::vector<size_t>& off);
+  void measure_clusters(const std::vector<ClusterTerm>& terms, double* values, double* sum);
   void compute_envs(const std::vector<int>& sites1, const std::vector<std::pair<int, int>>& sidelegs,
                     DevBuf& out1, DevBuf& out2, std::vector<size_t>& off2);
   void measure_terms(const std::vector<TermSpec>& terms, double* values, double* sum);

@@ -1021,12 +1021,25 @@ static void trim(std::string& s) {
   if (b < e) s.assign(b, e); else s.clear();
 }
 
-std::vector<PauliTerm> pauli_terms(const std::string& text, const Edges& edges, int64_t* n_dropped) {
-  std::vector<PauliTerm> out;
+namespace {
+struct PauliRow {
+  double re = 0, im = 0;
+  std::vector<std::pair<int, char>> ops;  // non-identity letters, ascending qubit
+};
+
+bool adjacent(const Edges& edges, int a, int b) {
+  for (int m : surrounding_bonds(edges, a)) {
+    const auto& e = edges[m];
+    if ((e.first == a && e.second == b) || (e.first == b && e.second == a)) return true;
+  }
+  return false;
+}
+
+std::vector<PauliRow> pauli_rows(const std::string& text) {
+  std::vector<PauliRow> rows;
   std::istringstream in(text);
   std::string line;
   size_t lineno = 0;
-  int64_t row = 0, dropped = 0;
   while (std::getline(in, line)) {
     ++lineno;
     trim(line);
@@ -1046,36 +1059,55 @@ std::vector<PauliTerm> pauli_terms(const std::string& text, const Edges& edges, 
         throw HostError(-5, "Invalid Pauli label: only I/X/Y/Z are allowed.");
     }
     // rightmost character is qubit 0; keep non-identity letters, ascending qubit
-    std::vector<std::pair<int, char>> ops;
+    PauliRow r;
+    r.re = re;
+    r.im = im;
     const size_t n = ps.size();
     for (size_t i = 0; i < n; ++i) {
       const char u = ps[n - 1 - i];
-      if (u != 'I') ops.push_back({(int)i, u});
+      if (u != 'I') r.ops.push_back({(int)i, u});
     }
+    rows.push_back(std::move(r));
+  }
+  return rows;
+}
+}  // namespace
+
+std::vector<PauliTerm> pauli_terms(const std::string& text, const Edges& edges, int64_t* n_dropped) {
+  std::vector<PauliTerm> out;
+  int64_t dropped = 0;
+  const auto rows = pauli_rows(text);
+  for (size_t row = 0; row < rows.size(); ++row) {
+    const auto& ops = rows[row].ops;
     PauliTerm t;
-    t.coeff_re = re;
-    t.coeff_im = im;
-    t.row = row++;
+    t.coeff_re = rows[row].re;
+    t.coeff_im = rows[row].im;
+    t.row = (int64_t)row;
     if (ops.size() == 1) {
       t.kind = 1; t.q0 = ops[0].first; t.q1 = -1; t.l0 = ops[0].second; t.l1 = 0;
       out.push_back(t);
-    } else if (ops.size() == 2) {
-      bool adj = false;
-      for (int m : surrounding_bonds(edges, ops[0].first)) {
-        const auto& e = edges[m];
-        if ((e.first == ops[0].first && e.second == ops[1].first) || (e.first == ops[1].first && e.second == ops[0].first)) { adj = true; break; }
-      }
-      if (adj) {
-        t.kind = 2; t.q0 = ops[0].first; t.q1 = ops[1].first; t.l0 = ops[0].second; t.l1 = ops[1].second;
-        out.push_back(t);
-      } else {
-        ++dropped;
-      }
+    } else if (ops.size() == 2 && adjacent(edges, ops[0].first, ops[1].first)) {
+      t.kind = 2; t.q0 = ops[0].first; t.q1 = ops[1].first; t.l0 = ops[0].second; t.l1 = ops[1].second;
+      out.push_back(t);
     } else {
       ++dropped;
     }
   }
   if (n_dropped) *n_dropped = dropped;
+  return out;
+}
+
+std::vector<PauliString> pauli_strings(const std::string& text, const Edges& edges) {
+  std::vector<PauliString> out;
+  for (const auto& r : pauli_rows(text)) {
+    PauliString t;
+    t.coeff_re = r.re;
+    t.coeff_im = r.im;
+    for (const auto& o : r.ops) { t.qubits.push_back(o.first); t.letters.push_back(o.second); }
+    const size_t k = r.ops.size();
+    t.kind = k == 0 ? 0 : k == 1 ? 1 : (k == 2 && adjacent(edges, r.ops[0].first, r.ops[1].first)) ? 2 : 3;
+    out.push_back(std::move(t));
+  }
   return out;
 }
 

@@ -38,6 +38,15 @@ struct PauliTerm {
   int64_t row = 0;
 };
 
+// Every row of a sparse-Pauli text: kind 0 identity, 1 one qubit, 2 a pair
+// on an edge (the two kinds ClassifyOps keeps), 3 any other product.
+struct PauliString {
+  int kind = 0;
+  std::vector<int> qubits;  // ascending
+  std::string letters;      // one per qubit
+  double coeff_re = 0, coeff_im = 0;
+};
+
 Edges square_lattice(int Lx, int Ly);
 std::vector<int> greedy_layering(const Edges& e, int* nlayers);
 std::vector<int> surrounding_bonds(const Edges& e, int site);
@@ -50,6 +59,7 @@ std::vector<Layer> qasm_tpo(const Program& p, const Edges& edges);
 Layer kicked_ising_tpo(const Edges& edges, double Jz, double hz, double hx, double dt);
 void opt_tpo_svd(const Edges& edges, Layer& layer, double eps);
 std::vector<PauliTerm> pauli_terms(const std::string& text, const Edges& edges, int64_t* n_dropped);
+std::vector<PauliString> pauli_strings(const std::string& text, const Edges& edges);
 std::vector<std::complex<double>> pauli_list(char letter);
 
 }  // namespace tnbp_host

@@ -79,6 +79,55 @@ static __global__ void __launch_bounds__(kThreads) k_terms(const TermTask* __res
   }
 }
 
+// Cluster measurement, one tree site: its Gram environment over (kept bond
+// leg t, physical leg p) contracted with the site's one-site operator,
+//   X[t + D t'] = sum_{p,p'} env[(t + D p) + C (t' + D p')] op[p + d p'],
+// C = D d; written in FP64 and, for absorption at the parent site, in
+// storage precision R.
+struct EnvOpTask {
+  const double2* env;
+  int D, d;            // d <= 2
+  double2 op[4];       // op[p + d p'] (reference layout)
+  double2* out64;      // D x D
+  void* out;           // D x D, storage precision (may be null)
+};
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_env_op(const EnvOpTask* __restrict__ tasks) {
+  using C = typename cvec<R>::type;
+  const EnvOpTask& tk = tasks[blockIdx.x];
+  const int D = tk.D, d = tk.d;
+  const long long CC = (long long)D * d;
+  for (long long idx = threadIdx.x; idx < (long long)D * D; idx += blockDim.x) {
+    const int t = (int)(idx % D), t2 = (int)(idx / D);
+    double2 acc = make_double2(0.0, 0.0);
+    for (int p = 0; p < d; ++p)
+      for (int p2 = 0; p2 < d; ++p2) acc = acc + tk.env[(t + D * p) + CC * (t2 + D * p2)] * tk.op[p + d * p2];
+    tk.out64[idx] = acc;
+    if (tk.out) static_cast<C*>(tk.out)[idx] = from_d2<C>(acc);
+  }
+}
+
+// out = sum_i a[i] b[i] (FP64, fixed order), one block per task: the two
+// halves of a tree cluster meeting on one bond, sum_{t,t'} X[t,t'] Y[t,t'].
+struct PairTask {
+  const double2* a;
+  const double2* b;
+  int n;
+  double2* out;
+};
+static __global__ void __launch_bounds__(kThreads) k_pair_dot(const PairTask* __restrict__ tasks) {
+  __shared__ double red[32];
+  const PairTask& tk = tasks[blockIdx.x];
+  double sr = 0.0, si = 0.0;
+  for (int i = threadIdx.x; i < tk.n; i += blockDim.x) {
+    const double2 v = tk.a[i] * tk.b[i];
+    sr += v.x; si += v.y;
+  }
+  sr = block_sum(sr, red);
+  si = block_sum(si, red);
+  if (threadIdx.x == 0) *tk.out = make_double2(sr, si);
+}
+
 // sum_k c_k <P_k> (FP64, one block, fixed order)
 static __global__ void k_weighted_sum(const TermTask* __restrict__ tasks, const double2* __restrict__ values,
                                int n, double2* out) {
