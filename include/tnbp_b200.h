@@ -273,7 +273,8 @@ int tnbp_measure_pauli_sum(tnbp_job* job, int64_t n_terms, const int32_t* kind,
    (include/tnbp/parser/paulitotpo.h:111-132: non-adjacent pairs, three or
    more qubits), which the reference does not measure.  Each term is
    measured on a tree cluster: the union of the shortest paths
-   (FindShortestPath, graph.h:57-108) from its first qubit to the others,
+   (FindShortestPath, graph.h:57-108) from its lowest-numbered qubit to the
+   others (independent of the order the qubits are listed in),
    contracted exactly with its ket and bra layers, the Pauli letters on the
    qubit sites and the BP messages on every leg leaving the tree;
    <P> = Z(P) / Z(identity).  Exact where the graph is a tree (BP messages are

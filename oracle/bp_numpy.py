@@ -323,8 +323,9 @@ def shortest_path(edges, src, dst):
 
 def cluster_tree(edges, qubits):
     """The tree cluster of a Pauli product on `qubits`: the union of the
-    shortest paths from qubits[0] to each other qubit, as {site: parent}
-    (the first qubit's parent is None)."""
+    shortest paths from the lowest-numbered qubit to each other qubit, as
+    {site: parent} (the root's parent is None)."""
+    qubits = sorted(qubits)
     parent = {qubits[0]: None}
     for q in qubits[1:]:
         path = shortest_path(edges, qubits[0], q)

@@ -1401,8 +1401,9 @@ void Job::measure_terms(const std::vector<TermSpec>& terms, double* values, doub
 // Pauli products on any set of distinct sites -- the terms ClassifyOps drops
 // (paulitotpo.h:111-132: pairs that are not adjacent, three or more qubits)
 // -- measured on a tree cluster T: the union of the shortest paths
-// (FindShortestPath, graph.h:57-108) from the first qubit's site to every
-// other qubit's site.  T's ket and bra layers, the term's Pauli on its qubit
+// (FindShortestPath, graph.h:57-108) from the lowest-numbered qubit's site to
+// every other qubit's site (so the cluster does not depend on the order in
+// which a term lists its qubits).  T's ket and bra layers, the term's Pauli on its qubit
 // sites and the incoming BP messages on every leg that leaves T are
 // contracted leaf to root: a tree site absorbs its children's results on
 // their legs (as BP messages are absorbed) and BP messages on its other
@@ -1432,9 +1433,15 @@ void Job::measure_clusters(const std::vector<ClusterTerm>& terms, double* values
   std::vector<std::vector<Node>> trees(terms.size());
   int max_height = 0;
   for (size_t i = 0; i < terms.size(); ++i) {
-    const auto& t = terms[i];
-    if (t.labels.size() < 2 || t.labels.size() != t.letters.size())
+    if (terms[i].labels.size() < 2 || terms[i].labels.size() != terms[i].letters.size())
       throw Error(TNBP_EINVAL, "a cluster term needs two or more qubits, one letter each");
+    ClusterTerm t = terms[i];  // qubits in ascending order: the first is the root
+    {
+      std::vector<std::pair<int, char>> q;
+      for (size_t k = 0; k < t.labels.size(); ++k) q.push_back({t.labels[k], t.letters[k]});
+      std::stable_sort(q.begin(), q.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+      for (size_t k = 0; k < q.size(); ++k) { t.labels[k] = q[k].first; t.letters[k] = q[k].second; }
+    }
     auto& nodes = trees[i];
     std::map<int, int> node_of;  // site -> node
     for (size_t k = 0; k < t.labels.size(); ++k) {

@@ -182,7 +182,7 @@ struct EnvReq {
 // A Pauli product on distinct sites measured on a tree cluster (see
 // Job::measure_clusters).
 struct ClusterTerm {
-  std::vector<int> labels;  // site labels of the qubits; the first is the tree root
+  std::vector<int> labels;  // site labels of the qubits (the lowest is the tree root)
   std::vector<char> letters;
   double coeff[2];
 };
