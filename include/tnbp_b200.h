@@ -153,6 +153,13 @@ int tnbp_job_create(const int32_t* edges, int64_t n_edges, const int32_t* phys_d
                     int32_t precision, void* stream, uint64_t hbm_budget_bytes, tnbp_job** out);
 int tnbp_job_destroy(tnbp_job* job);
 int tnbp_job_info(const tnbp_job* job, int64_t* n_sites, int64_t* n_edges, int32_t* precision);
+/* Estimated peak device bytes of a job on this edge list whose BP runs at
+   bond dimension bond_dim[e] on edge e (the largest it reaches; physical
+   dimension 2): site tensors with their spare, chain and sweep-scratch
+   buffers, message arenas, truncation work; the figure the server admits
+   requests by.  Host only. */
+int tnbp_footprint_estimate(const int32_t* edges, int64_t n_edges, const int32_t* bond_dim,
+                            int32_t precision, uint64_t* bytes_out);
 /* Bytes of device memory the job holds now. */
 int tnbp_job_device_bytes(const tnbp_job* job, uint64_t* bytes);
 /* Current bond dimension of every edge (n_edges ints). */

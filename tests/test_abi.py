@@ -39,3 +39,19 @@ def test_no_oracle_on_the_product_path():
             if f.endswith((".py", ".cu", ".cuh", ".cpp", ".h")):
                 txt = open(os.path.join(dp, f), errors="ignore").read()
                 assert "bp_numpy" not in txt and "gqten_cpu" not in txt, f
+
+
+def test_footprint_estimate_host_only():
+    """tnbp_footprint_estimate (the server's admission figure) runs without a
+    device: exact on a one-edge graph, ordered by precision, growing with D."""
+    tb = pytest.importorskip("tnbp_b200")
+    one = tb.footprint_estimate([(0, 1)], [1], tb.C128)
+    # two degree-1 sites of 2 elements x (4 x 16 B); one edge: arenas 128 B,
+    # truncation 128 B, Gram partials 512 B; x 1.1 plus 8 MiB
+    assert one == int((2 * 2 * 64 + 128 + 128 + 512) * 1.1) + (8 << 20)
+    e = tb.bond_square_lattice(6, 6)
+    f = {p: tb.footprint_estimate(e, [16] * len(e), p) for p in (tb.C64, tb.MIXED, tb.C128)}
+    assert f[tb.C64] < f[tb.MIXED] < f[tb.C128]
+    assert tb.footprint_estimate(e, [32] * len(e), tb.MIXED) > 8 * f[tb.MIXED]
+    with pytest.raises(tb.TnbpError):
+        tb.footprint_estimate(e, [0] * len(e), tb.MIXED)

@@ -66,6 +66,7 @@ _SIGS = {
     "tnbp_job_destroy": [_vp],
     "tnbp_job_info": [_vp, _i64p, _i64p, _i32p],
     "tnbp_job_device_bytes": [_vp, _u64p],
+    "tnbp_footprint_estimate": [_i32p, C.c_int64, _i32p, C.c_int32, _u64p],
     "tnbp_bond_dims": [_vp, _i32p],
     "tnbp_site_shape": [_vp, C.c_int64, _i32p, C.c_int32, _i32p],
     "tnbp_download_site": [_vp, C.c_int64, _f64p, C.c_int64],
@@ -360,6 +361,16 @@ def LoadTPS(path, edges):
         E.append(mdata[o:o + D * D].reshape((D, D), order="F").copy())
         o += D * D
     return V, E
+
+
+def footprint_estimate(edges, bond_dims, precision=C128):
+    """Estimated peak device bytes of a job on `edges` with BP at the given
+    bond dimension per edge (tnbp_footprint_estimate; host only)."""
+    e = _edges_arr(edges)
+    d = np.ascontiguousarray(bond_dims, np.int32)
+    out = C.c_uint64()
+    _chk(lib.tnbp_footprint_estimate(_p(e, _i32p), len(e), _p(d, _i32p), precision, C.byref(out)))
+    return out.value
 
 
 # ------------------------------------------------------------------ state

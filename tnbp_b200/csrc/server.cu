@@ -65,28 +65,18 @@ static int sweep_slots(int g) {
   return g + sweep_slots(h) + sweep_slots(g - h);
 }
 
-// Peak device bytes of a request.  Bond dimension during BP on edge e: at
-// most chi times the largest TPO rank on e, and at most the product of the
-// ranks absorbed since |0...0>.  Per site the tensor, its spare buffer, the
-// two chain buffers of truncation, the complex64 sweep copy (TNBP_MIXED) and
-// the sweep scratch slots of its degree; both message arenas twice; per-edge
-// truncation work and Gram partials; the request's TPO layers.
-uint64_t Server::footprint(const Request& r) const {
+// Peak device bytes of a job on `edges` whose BP runs at bond dimension
+// D[e] on edge e (physical dimension 2): per site the tensor, its spare
+// buffer, the two chain buffers of truncation, the complex64 sweep copy
+// (TNBP_MIXED) and the sweep scratch slots of its degree; both message arenas
+// twice; per-edge truncation work and Gram partials; plus extra_bytes; 10 %
+// and 8 MiB of margin.
+uint64_t footprint_estimate(const std::vector<std::pair<int, int>>& edges, const std::vector<double>& D, int prec,
+                            uint64_t extra_bytes) {
   const double esz = prec == TNBP_C64 ? 8.0 : 16.0;   // stored element
   const double wsz = prec == TNBP_C128 ? 16.0 : 8.0;  // sweep element
   const double shadow = prec == TNBP_MIXED ? 8.0 : 0.0;
-  const TpoSet& ts = *r.tpos;
-  const auto& edges = ts.edges;
   const size_t ne = edges.size();
-  const int nsteps = r.source == Request::QASM ? (int)ts.layers.size() : r.steps;
-  std::vector<double> D(ne);
-  for (size_t e = 0; e < ne; ++e) {
-    const double cap = (double)r.chi * ts.rank_max[e];
-    double prod = 1.0;
-    for (int t = 0; t < nsteps && prod < cap; ++t)
-      prod *= ts.layers[r.source == Request::QASM ? t : 0]->rank[e];
-    D[e] = std::max(1.0, std::min(cap, prod));
-  }
   const auto sites = tnbp_host::site_labels(edges);
   std::map<int, size_t> pos;
   for (size_t i = 0; i < sites.size(); ++i) pos[sites[i]] = i;
@@ -106,8 +96,27 @@ uint64_t Server::footprint(const Request& r) const {
     bytes += 8.0 * dd * 16.0;        // truncation work
     bytes += 2.0 * 16.0 * dd * 16.0; // Gram partials (upper bound)
   }
-  bytes += (double)ts.device_bytes;
+  bytes += (double)extra_bytes;
   return (uint64_t)(bytes * 1.1) + (8ull << 20);
+}
+
+// Peak device bytes of a request.  Bond dimension during BP on edge e: at
+// most chi times the largest TPO rank on e, and at most the product of the
+// ranks absorbed since |0...0>; plus the request's TPO layers.
+uint64_t Server::footprint(const Request& r) const {
+  const TpoSet& ts = *r.tpos;
+  const auto& edges = ts.edges;
+  const size_t ne = edges.size();
+  const int nsteps = r.source == Request::QASM ? (int)ts.layers.size() : r.steps;
+  std::vector<double> D(ne);
+  for (size_t e = 0; e < ne; ++e) {
+    const double cap = (double)r.chi * ts.rank_max[e];
+    double prod = 1.0;
+    for (int t = 0; t < nsteps && prod < cap; ++t)
+      prod *= ts.layers[r.source == Request::QASM ? t : 0]->rank[e];
+    D[e] = std::max(1.0, std::min(cap, prod));
+  }
+  return footprint_estimate(edges, D, prec, ts.device_bytes);
 }
 
 // The TPO layers of a circuit, built and uploaded on the first request that
@@ -430,6 +439,23 @@ int tnbp_server_submit_qasm(tnbp_server* srv, const char* qasm_src, const char* 
     }
     const int64_t id = srv->s->submit(std::move(r));
     if (request_id) *request_id = id;
+  });
+}
+
+int tnbp_footprint_estimate(const int32_t* edges, int64_t n_edges, const int32_t* bond_dim, int32_t precision,
+                            uint64_t* bytes) {
+  return sguard([&] {
+    if (!bytes || !bond_dim || (n_edges > 0 && !edges)) throw tnbp::Error(TNBP_EINVAL, "NULL argument");
+    if (precision != TNBP_C128 && precision != TNBP_C64 && precision != TNBP_MIXED)
+      throw tnbp::Error(TNBP_EINVAL, "unknown precision");
+    std::vector<std::pair<int, int>> e(n_edges);
+    std::vector<double> D(n_edges);
+    for (int64_t i = 0; i < n_edges; ++i) {
+      e[i] = {edges[2 * i], edges[2 * i + 1]};
+      if (bond_dim[i] < 1) throw tnbp::Error(TNBP_EINVAL, "bond dimension < 1");
+      D[i] = bond_dim[i];
+    }
+    *bytes = tnbp::footprint_estimate(e, D, precision, 0);
   });
 }
 

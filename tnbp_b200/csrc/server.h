@@ -25,6 +25,9 @@ struct TpoSet {
   uint64_t device_bytes = 0;
 };
 
+uint64_t footprint_estimate(const std::vector<std::pair<int, int>>& edges, const std::vector<double>& D, int prec,
+                            uint64_t extra_bytes);
+
 struct Request {
   enum Phase { QUEUED, ABSORB, BP, TRUNC, MEASURE, DONE };
   // KICKED_ISING: the one layer of tpos applied `steps` times; QASM: the
