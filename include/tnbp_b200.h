@@ -42,6 +42,7 @@ extern "C" {
 #define TNBP_EPARSE -5      /* QASM / Pauli text parse error (qasm::ParseError, runtime_error) */
 #define TNBP_EUNSUPPORTED -6 /* gate or operator the reference also rejects */
 #define TNBP_ENOGPU -7      /* no CUDA device visible */
+#define TNBP_ECANCELED -8   /* the request was cancelled (tnbp_server_cancel) */
 
 /* ---- precision of a job's device state ---- */
 #define TNBP_C128 0 /* plain path: complex128 storage and arithmetic */
@@ -381,6 +382,11 @@ int tnbp_server_submit_qasm(tnbp_server* srv, const char* qasm_src, const char* 
    programs held now. */
 int tnbp_server_tpo_cache_stats(tnbp_server* srv, int64_t* hits_out, int64_t* misses_out,
                                 int64_t* entries_out);
+/* Cancel a request that has not finished: a queued one leaves the queue, an
+   admitted one releases its device state and its share of the HBM budget at
+   once (between server steps, so none of its work is in flight).  It is then
+   done with TNBP_ECANCELED; cancelling a finished request is a no-op. */
+int tnbp_server_cancel(tnbp_server* srv, int64_t request_id);
 /* Advance the loop once (admission + one batched stage).  n_done_out =
    number of requests that completed during this call. */
 int tnbp_server_step(tnbp_server* srv, int32_t* n_active_out, int32_t* n_queued_out,

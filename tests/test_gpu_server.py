@@ -135,3 +135,37 @@ def test_admission_rejects_a_request_larger_than_the_budget():
         assert e.value.code == tb.ENOMEM
     finally:
         srv.close()
+
+
+def test_cancelled_requests_leave_the_others_unchanged():
+    """tnbp_server_cancel between steps: a queued request and an admitted one
+    are cancelled (TNBP_ECANCELED); the remaining request's result equals its
+    result alone, and the freed slot admits the next queued request."""
+    _need_gpu()
+    keep, drop_active, drop_queued, later = REQUESTS[0], REQUESTS[1], REQUESTS[2], REQUESTS[4]
+    alone = run_server([keep], tb.MIXED)[0]
+    alone_later = run_server([later], tb.MIXED)[0]
+    srv = tb.Server(tb.MIXED, 0, 2)
+    try:
+        ids = []
+        for L, chi, nst, th, seed in (keep, drop_active, drop_queued, later):
+            ids.append(srv.submit_kicked_ising(L, chi, nst, THETA_J, th, observable(L, seed)))
+        srv.step()
+        srv.step()  # two admitted (slot limit 2), two queued
+        srv.cancel(ids[1])
+        srv.cancel(ids[2])
+        steps = 0
+        while srv.result(ids[0]) is None or srv.result(ids[3]) is None:
+            srv.step()
+            steps += 1
+            assert steps < 100000
+        for i in (1, 2):
+            with pytest.raises(tb.TnbpError) as e:
+                srv.result(ids[i])
+            assert e.value.code == tb.ECANCELED
+        assert abs(srv.result(ids[0]) - alone) <= TOL_MIX
+        assert abs(srv.result(ids[3]) - alone_later) <= TOL_MIX
+        srv.cancel(ids[0])  # finished: no-op
+        assert abs(srv.result(ids[0]) - alone) <= TOL_MIX
+    finally:
+        srv.close()

@@ -19,7 +19,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libtnbp_b200.so")
 
 C128, C64, MIXED = 0, 1, 2
-OK, EINVAL, ECUDA, ENOMEM, ENOTCONV, EPARSE, EUNSUPPORTED, ENOGPU = 0, -1, -2, -3, -4, -5, -6, -7
+OK, EINVAL, ECUDA, ENOMEM, ENOTCONV, EPARSE, EUNSUPPORTED, ENOGPU, ECANCELED = 0, -1, -2, -3, -4, -5, -6, -7, -8
 
 
 class TnbpError(RuntimeError):
@@ -95,6 +95,7 @@ _SIGS = {
     "tnbp_server_submit_qasm": [_vp, C.c_char_p, C.c_char_p, C.c_int32, C.c_double, C.c_int32, C.c_double,
                                 C.c_int32, C.c_double, _i64p],
     "tnbp_server_tpo_cache_stats": [_vp, _i64p, _i64p, _i64p],
+    "tnbp_server_cancel": [_vp, C.c_int64],
     "tnbp_server_step": [_vp, _i32p, _i32p, _i32p],
     "tnbp_server_result": [_vp, C.c_int64, _f64p, _i32p],
 }
@@ -635,6 +636,10 @@ class Server:
         h, m, e = C.c_int64(), C.c_int64(), C.c_int64()
         _chk(lib.tnbp_server_tpo_cache_stats(self.h, C.byref(h), C.byref(m), C.byref(e)))
         return h.value, m.value, e.value
+
+    def cancel(self, rid):
+        """Cancel a request that has not finished (tnbp_server_cancel)."""
+        _chk(lib.tnbp_server_cancel(self.h, rid))
 
     def step(self):
         a, q, d = C.c_int32(), C.c_int32(), C.c_int32()

@@ -48,7 +48,8 @@ def build(verbose=True, jobs=4):
             cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                    "--expt-relaxed-constexpr", "-c", src, "-o", obj]
         else:
-            cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-c", src, "-o", obj]
+            cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-I", os.path.join(os.path.dirname(os.path.dirname(NVCC)),
+                                                                        "include"), "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         procs.append((subprocess.Popen(cmd), cmd))

@@ -465,6 +465,7 @@ int tnbp_tpo_create(tnbp_job* job, const int32_t* edge_rank, const int64_t* op_o
       t->dout[s] = J.pd[s];
       total = std::max(total, t->op_offset[s] + n);
     }
+    for (int64_t i = 0; i < 2 * total; ++i) need(std::isfinite(op_data[i]), "non-finite TPO element");
     t->ops.alloc((size_t)total * sizeof(double2), J.stream);
     CK(cudaMemcpyAsync(t->ops.p, op_data, (size_t)total * sizeof(double2), cudaMemcpyHostToDevice, J.stream));
     CK(cudaStreamSynchronize(J.stream));

@@ -815,6 +815,11 @@ struct LayerBuilder {
     }
   }
   void append(const Instruction& in) {
+    // the reference builds NaN operators from an infinite angle (strtod of
+    // "1e400") without complaint; here the layer is refused before it can
+    // reach the device
+    for (double p : in.params)
+      if (!std::isfinite(p)) throw HostError(-1, "non-finite gate parameter");
     const auto U = gate_matrix(in);
     const int nq = qubit_count(in);
     if (nq == 1) one_qubit((int)in.qubits[0].index, U);
@@ -862,6 +867,8 @@ std::vector<Layer> qasm_tpo(const Program& p, const Edges& edges) {
 // exp(-i th ZZ) = cos(th) I(x)I - i sin(th) Z(x)Z, split term by term with
 // the magnitude shared evenly between the two sites.
 Layer kicked_ising_tpo(const Edges& edges, double Jz, double hz, double hx, double dt) {
+  if (!std::isfinite(Jz) || !std::isfinite(hz) || !std::isfinite(hx) || !std::isfinite(dt))
+    throw HostError(-1, "non-finite kicked-Ising parameter");
   LayerBuilder lb(edges);
   const double th = dt * Jz;
   const cd I(0, 1);
@@ -932,7 +939,11 @@ void opt_tpo_svd(const Edges& edges, Layer& layer, double eps) {
     const int64_t off = layer.op_offset[si];
     if (off < 0 || off + n > avail) throw HostError(-1, "TPO site operator outside the op data");
     o.data.resize(n);
-    for (int64_t x = 0; x < n; ++x) o.data[x] = cd(layer.op_data[2 * (off + x)], layer.op_data[2 * (off + x) + 1]);
+    for (int64_t x = 0; x < n; ++x) {
+      o.data[x] = cd(layer.op_data[2 * (off + x)], layer.op_data[2 * (off + x) + 1]);
+      if (!std::isfinite(o.data[x].real()) || !std::isfinite(o.data[x].imag()))
+        throw HostError(-1, "non-finite TPO element");
+    }
   }
 
   for (size_t m = 0; m < ne; ++m) {

@@ -232,6 +232,18 @@ void Server::fail(Request& r, int code, const std::string& msg) {
   r.phase = Request::DONE;
 }
 
+void Server::cancel(int64_t id) {
+  auto it = reqs.find(id);
+  if (it == reqs.end()) throw Error(TNBP_EINVAL, "unknown request id");
+  Request& r = *it->second;
+  if (r.phase == Request::DONE) return;
+  const bool admitted = r.phase != Request::QUEUED;
+  queue.erase(std::remove(queue.begin(), queue.end(), id), queue.end());
+  active.erase(std::remove(active.begin(), active.end(), id), active.end());
+  if (admitted) in_use -= r.footprint;
+  fail(r, TNBP_ECANCELED, "request cancelled");
+}
+
 void Server::step(int* n_active, int* n_queued, int* n_done) {
   TNBP_TRACE_SCOPE("server.step");
   int done = 0;
@@ -390,6 +402,10 @@ int tnbp_server_submit_kicked_ising(tnbp_server* srv, int32_t L, int32_t chi, in
     for (int64_t i = 0; i < n_terms; ++i)
       if (r->kind[i] != 1 && r->kind[i] != 2) throw tnbp::Error(TNBP_EINVAL, "term kind must be 1 or 2");
     if (L < 2) throw tnbp::Error(TNBP_EINVAL, "lattice side must be >= 2");
+    if (!std::isfinite(theta_j) || !std::isfinite(theta_h) || !std::isfinite(bp_tol) || !std::isfinite(sv_min))
+      throw tnbp::Error(TNBP_EINVAL, "non-finite request parameter");
+    for (int64_t i = 0; i < 2 * n_terms; ++i)
+      if (!std::isfinite(coeff[i])) throw tnbp::Error(TNBP_EINVAL, "non-finite term coefficient");
     // RZZ(theta_j) = exp(-i theta_j/2 ZZ), RX(theta_h) = exp(-i theta_h/2 X)
     char key[96];
     std::snprintf(key, sizeof(key), "kicked_ising %d %a %a", L, theta_j, theta_h);
@@ -408,6 +424,8 @@ int tnbp_server_submit_qasm(tnbp_server* srv, const char* qasm_src, const char* 
   return sguard([&] {
     if (!srv) throw tnbp::Error(TNBP_EINVAL, "server is NULL");
     if (!qasm_src || !pauli_text) throw tnbp::Error(TNBP_EINVAL, "NULL program or observable");
+    if (!std::isfinite(bp_tol) || !std::isfinite(sv_min) || !std::isfinite(eps_opt_tpo))
+      throw tnbp::Error(TNBP_EINVAL, "non-finite request parameter");
     auto r = std::make_unique<tnbp::Request>();
     r->source = tnbp::Request::QASM;
     r->chi = chi; r->tol = bp_tol; r->maxit = bp_max_iter; r->sv_min = sv_min;
@@ -476,6 +494,13 @@ int tnbp_server_step(tnbp_server* srv, int32_t* n_active, int32_t* n_queued, int
     if (n_active) *n_active = a;
     if (n_queued) *n_queued = q;
     if (n_done) *n_done = d;
+  });
+}
+
+int tnbp_server_cancel(tnbp_server* srv, int64_t id) {
+  return sguard([&] {
+    if (!srv) throw tnbp::Error(TNBP_EINVAL, "server is NULL");
+    srv->s->cancel(id);
   });
 }
 

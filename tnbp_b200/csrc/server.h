@@ -82,6 +82,7 @@ struct Server {
   void start(Request& r);
   void finish(Request& r);
   void fail(Request& r, int code, const std::string& msg);
+  void cancel(int64_t id);
 };
 
 }  // namespace tnbp

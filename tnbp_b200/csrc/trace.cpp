@@ -1,5 +1,7 @@
 #include "trace.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <cstdio>
 #include <cstdlib>
 #include <map>
@@ -32,6 +34,17 @@ bool trace_enabled() {
   }();
   return on;
 }
+
+bool nvtx_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("TNBP_NVTX");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+void nvtx_push(const char* name) { nvtxRangePushA(name); }
+void nvtx_pop() { nvtxRangePop(); }
 
 void trace_add(const char* name, double seconds) {
   Totals& tt = totals();
