@@ -17,8 +17,9 @@
    codes): TNBP_EPARSE -> ParseError (a std::runtime_error, as
    qasm::ParseError, include/qasm/ir.h:36-41, and the sparse-Pauli reader's
    runtime_error); TNBP_EINVAL -> std::invalid_argument; TNBP_ENOMEM ->
-   std::bad_alloc; anything else -> std::runtime_error with the engine's
-   message. */
+   std::bad_alloc; TNBP_ENOTCONV -> NotConverged; anything else (a
+   cancelled request, CUDA errors, no device) -> std::runtime_error with
+   the engine's message. */
 #pragma once
 
 #include <algorithm>
@@ -389,5 +390,67 @@ inline cplx MeasurePauliText(State& W, const std::string& sparse_pauli_text, std
    make_rank_filename(prefix, 0) is prefix + "000000.dat"). */
 inline void SaveTPS(State& W, const std::string& filename) { check(tnbp_save_state(W.handle(), filename.c_str())); }
 inline void LoadTPS(State& W, const std::string& filename) { check(tnbp_load_state(W.handle(), filename.c_str())); }
+
+/* ---------------------------------------------------- served requests */
+
+/* The continuous-batching estimator server (tnbp_server_*): requests queue
+   and are admitted by HBM footprint; every step() runs one batched BP sweep
+   over all admitted requests.  result() is empty while a request runs and
+   throws the request's own error (NotConverged, ..., or std::runtime_error
+   for a cancelled one) if it failed. */
+class Server {
+ public:
+  explicit Server(int precision = TNBP_MIXED, uint64_t hbm_budget_bytes = 0, int max_active = 64) {
+    check(tnbp_server_create(precision, hbm_budget_bytes, max_active, &srv_));
+  }
+  ~Server() {
+    if (srv_) tnbp_server_destroy(srv_);
+  }
+  Server(const Server&) = delete;
+  Server& operator=(const Server&) = delete;
+
+  /* Kicked Ising on an L x L lattice: n_steps of RZZ(theta_j) on every edge
+     then RX(theta_h), BP to bp_tol / bp_max_iter, truncation to chi;
+     observable = ClassifyOps' kept terms of `terms`. */
+  int64_t submit_kicked_ising(int L, int chi, int n_steps, double theta_j, double theta_h, const PauliTerms& terms,
+                              double bp_tol = 1e-8, int bp_max_iter = 50, double sv_min = 1e-8) {
+    int64_t id = 0;
+    check(tnbp_server_submit_kicked_ising(srv_, L, chi, n_steps, theta_j, theta_h, bp_tol, bp_max_iter, sv_min,
+                                          (int64_t)terms.size(), terms.kind.data(), terms.q0.data(),
+                                          terms.q1.data(), terms.letters.data(),
+                                          reinterpret_cast<const double*>(terms.coeff.data()), &id));
+    return id;
+  }
+  /* The estimator app's workload: a QASM program and a sparse-Pauli text. */
+  int64_t submit_qasm(const std::string& qasm_source, const std::string& sparse_pauli_text, int chi,
+                      double bp_tol = 1e-8, int bp_max_iter = 50, double sv_min = 1e-8, bool do_opt_tpo = false,
+                      double eps_opt_tpo = 1e-8) {
+    int64_t id = 0;
+    check(tnbp_server_submit_qasm(srv_, qasm_source.c_str(), sparse_pauli_text.c_str(), chi, bp_tol, bp_max_iter,
+                                  sv_min, do_opt_tpo ? 1 : 0, eps_opt_tpo, &id));
+    return id;
+  }
+  /* One server step; returns the number of requests that finished in it. */
+  int step(int* n_active = nullptr, int* n_queued = nullptr) {
+    int32_t a = 0, q = 0, d = 0;
+    check(tnbp_server_step(srv_, &a, &q, &d));
+    if (n_active) *n_active = a;
+    if (n_queued) *n_queued = q;
+    return d;
+  }
+  /* true and the request's sum_k c_k <P_k> once it has finished. */
+  bool result(int64_t id, cplx* sum) {
+    double v[2] = {0.0, 0.0};
+    int32_t pending = 1;
+    check(tnbp_server_result(srv_, id, v, &pending));
+    if (pending) return false;
+    if (sum) *sum = cplx(v[0], v[1]);
+    return true;
+  }
+  void cancel(int64_t id) { check(tnbp_server_cancel(srv_, id)); }
+
+ private:
+  tnbp_server* srv_ = nullptr;
+};
 
 }  // namespace tnbp_b200

@@ -73,7 +73,9 @@ int main() {
   EXPECT(throws<std::runtime_error>([&] { tb::QasmToTPO("OPENQASM 2.0;\nqreg q[3];\nccx q[0],q[1],q[2];\n", qe); }),
          "runtime_error on an unsupported gate");
   EXPECT(throws<std::invalid_argument>([&] { tb::bond_square_lattice(0, 3); }), "invalid_argument on bad sizes");
-  if (!tnbp_device_available())
+  if (!tnbp_device_available()) {
     EXPECT(throws<std::runtime_error>([&] { tb::State s(e); }), "no device: State refuses (no CPU path)");
+    EXPECT(throws<std::runtime_error>([&] { tb::Server s; }), "no device: Server refuses (no CPU path)");
+  }
   return 0;
 }
