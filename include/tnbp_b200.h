@@ -119,6 +119,18 @@ int tnbp_qasm_tpo(const char* qasm_src, const int32_t* edges, int64_t n_edges,
                   int32_t* edge_rank, int64_t* op_offset, double* op_data, int64_t cap_elems,
                   int32_t* n_layers_out, int64_t* n_elems_out);
 
+/* QasmToTPO with manual gate-number layering (qasmtotpo.h:709-738, the
+   estimator app's --num_gates): layer m takes the next num_gates[m]
+   instructions; same output layout as tnbp_qasm_tpo.  A barrier, measure,
+   reset or custom gate is TNBP_EUNSUPPORTED (the reference throws "matrix
+   for this op not implemented"); more instructions than the counts cover,
+   a layer that receives none, or a count < 1 is TNBP_EINVAL (undefined in
+   the reference). */
+int tnbp_qasm_tpo_counts(const char* qasm_src, const int32_t* edges, int64_t n_edges,
+                         const int32_t* num_gates, int32_t n_counts, int32_t* edge_rank,
+                         int64_t* op_offset, double* op_data, int64_t cap_elems,
+                         int32_t* n_layers_out, int64_t* n_elems_out);
+
 /* Kicked-Ising Floquet step as one TPO layer: exp(-i dt Jz ZZ) on every
    edge in edge order, then exp(-i dt hz Z), then exp(-i dt hx X) on every
    site (apps/kicked_ising_lattice/circuit.h:14-229).  The two-site gate is

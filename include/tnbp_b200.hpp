@@ -168,6 +168,33 @@ inline std::vector<TpoLayer> QasmToTPO(const std::string& qasm_source, const Edg
   return out;
 }
 
+/* QasmToTPO with manual gate-number layering (qasmtotpo.h:709-738):
+   layer m takes the next num_gates[m] instructions. */
+inline std::vector<TpoLayer> QasmToTPO(const std::string& qasm_source, const Edges& edges,
+                                       const std::vector<int>& num_gates) {
+  const auto f = detail::flat(edges);
+  const std::vector<int32_t> ng(num_gates.begin(), num_gates.end());
+  const int64_t ne = (int64_t)edges.size(), ns = (int64_t)GetSiteIndexFromBond(edges).size();
+  int32_t nl = 0;
+  int64_t nel = 0;
+  check(tnbp_qasm_tpo_counts(qasm_source.c_str(), f.data(), ne, ng.data(), (int32_t)ng.size(), nullptr, nullptr,
+                             nullptr, 0, &nl, &nel));
+  std::vector<int32_t> rank((size_t)nl * ne + 1);
+  std::vector<int64_t> off((size_t)nl * ns + 1);
+  std::vector<cplx> data((size_t)nel + 1);
+  check(tnbp_qasm_tpo_counts(qasm_source.c_str(), f.data(), ne, ng.data(), (int32_t)ng.size(), rank.data(),
+                             off.data(), reinterpret_cast<double*>(data.data()), nel, &nl, &nel));
+  std::vector<TpoLayer> out(nl);
+  for (int32_t l = 0; l < nl; ++l) {
+    const int64_t base = off[(size_t)l * ns];
+    const int64_t end = l + 1 < nl ? off[(size_t)(l + 1) * ns] : nel;
+    out[l].edge_rank.assign(rank.begin() + (size_t)l * ne, rank.begin() + (size_t)(l + 1) * ne);
+    for (int64_t s = 0; s < ns; ++s) out[l].op_offset.push_back(off[(size_t)l * ns + s] - base);
+    out[l].op_data.assign(data.begin() + base, data.begin() + end);
+  }
+  return out;
+}
+
 /* OptTPObySVD (include/tnbp/ptns/function/optsvdtpo.h:86-214), in place. */
 inline void OptTPObySVD(const Edges& edges, TpoLayer& O, double eps) {
   const auto f = detail::flat(edges);

@@ -8,6 +8,8 @@
 // usage: ref_hostparity lattice <Lx> <Ly>
 //        ref_hostparity qasm <file.qasm> [<pauli.txt> [<Lx> <Ly>]]
 //        ref_hostparity opttpo <file.qasm> <eps> [<Lx> <Ly>]
+//        ref_hostparity tpocount <file.qasm> <n0,n1,...>
+// (tpocount: QasmToTPO with manual gate-number layering, qasmtotpo.h:709-738)
 // (opttpo: every TPO layer of QasmToTPO before and after the reference's
 //  OptTPObySVD, include/tnbp/ptns/function/optsvdtpo.h, as shapes and
 //  column-major element lists)
@@ -105,6 +107,20 @@ int main(int argc, char** argv) {
     std::printf(", ");
     tpo_json("after", T);
     std::printf(", \"eps\": %.17g, \"opt_seconds\": %.6g", eps, secs);
+  } else if (mode == "tpocount") {
+    auto prog = qasm::parse_any(qasm::read_all_file(argv[2]));
+    std::vector<int> counts;
+    {
+      std::stringstream ss(argv[3]);
+      std::string tok;
+      while (std::getline(ss, tok, ',')) counts.push_back(std::stoi(tok));
+    }
+    auto edges = tnbp::EdgesFromQasm(prog);
+    edges_json("edges", edges);
+    tci::gqten_handle ctx;
+    auto T = tnbp::QasmToTPO<Tensor>(ctx, prog, edges, counts);
+    std::printf(", ");
+    tpo_json("layers", T);
   } else if (mode == "qasm") {
     auto prog = qasm::parse_any(qasm::read_all_file(argv[2]));
     std::printf("\"instructions\": [");

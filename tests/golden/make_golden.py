@@ -19,6 +19,9 @@ oracle/_ref/, and this script runs them on seeded synthetic inputs:
                      to gauge-invariant data (bond dimensions, per-leg
                      singular values of every site operator)
   opt_<name>.json    the estimator app's printed values with --do_opt_tpo 1
+  tpocount_<name>.npz  TPO layers of the reference's manual gate-number
+                     layering (QasmToTPO with num_gates) for several splits
+  count_<name>.json  the estimator app's printed values with --num_gates
   ckpt_<name>000000.dat + ckpt_<name>.json
                      a checkpoint the reference's estimator_restart app saved
                      after one pass of a circuit (SaveTPS, iotps.h) and the
@@ -198,6 +201,53 @@ def run_opt_estimator(name, qasm, pauli, chi, sv_min, tol, maxit, eps):
     with open(os.path.join(HERE, f"opt_{name}.json"), "w") as f:
         json.dump(res, f, indent=1)
     print(f"opt_{name}: {len(one)} one-site, {len(two)} two-site values, conditions {conds}")
+
+
+def kicked_ising_no_barrier(Lx, Ly, steps, theta_j, theta_h):
+    """kicked_ising_qasm without barriers (manual layering counts instructions)."""
+    return "\n".join(l for l in kicked_ising_qasm(Lx, Ly, steps, theta_j, theta_h).splitlines()
+                     if not l.startswith("barrier")) + "\n"
+
+
+def run_tpocount(name, qasm, splits):
+    qp = os.path.join(INPUTS, f"{name}.qasm")
+    with open(qp, "w") as f:
+        f.write(qasm)
+    arrays = {}
+    for k, split in enumerate(splits):
+        arg = ",".join(str(n) for n in split)
+        d = json.loads(subprocess.check_output([os.path.join(REF_BIN, "ref_hostparity"), "tpocount", qp, arg],
+                                               text=True))
+        arrays["edges"] = np.array(d["edges"], np.int32)
+        arrays[f"split{k}"] = np.array(split, np.int32)
+        for l, layer in enumerate(d["layers"]):
+            for s_, (shape, flat) in enumerate(layer):
+                a = np.array(flat, np.float64).reshape(-1, 2)
+                arrays[f"split{k}/{l}/{s_}"] = (a[:, 0] + 1j * a[:, 1]).reshape(shape, order="F")
+    np.savez_compressed(os.path.join(HERE, f"tpocount_{name}.npz"), **arrays)
+    print(f"tpocount_{name}: {len(splits)} splits")
+
+
+def run_count_estimator(name, qasm, pauli, chi, sv_min, tol, maxit, split):
+    """The reference estimator app with --num_gates: its printed values."""
+    qp = os.path.join(INPUTS, f"{name}.qasm")
+    pp = os.path.join(INPUTS, f"{name}.txt")
+    with open(qp, "w") as f:
+        f.write(qasm)
+    with open(pp, "w") as f:
+        f.write(pauli)
+    out = subprocess.check_output(
+        [os.path.join(REF_BIN, "estimator"), "--circuit", qp, "--sparse_pauli", pp, "--max_bond_dim", str(chi),
+         "--bp_tolerance", repr(tol), "--max_bp_iterations", str(maxit), "--sv_min", repr(sv_min),
+         "--num_gates", ",".join(str(n) for n in split)], text=True)
+    one = [float(v) for v in re.findall(r"single site operator at site \d+ (\S+)", out)]
+    two = [float(v) for v in re.findall(r"two site operator at sites \(\d+,\d+\) (\S+)", out)]
+    dims = [int(v) for v in re.findall(r"bond dim = (\d+)", out)]
+    res = dict(chi=chi, sv_min=sv_min, tol=tol, maxit=maxit, num_gates=list(split), one=one, two=two,
+               bond_dims=dims)
+    with open(os.path.join(HERE, f"count_{name}.json"), "w") as f:
+        json.dump(res, f, indent=1)
+    print(f"count_{name}: {len(one)} one-site, {len(two)} two-site values")
 
 
 def run_checkpoint(name, qasm, pauli, chi, sv_min, tol, maxit, nlayers):
@@ -404,6 +454,12 @@ def main():
         orng = np.random.default_rng(20261204)
         q = zz_cx_qasm(3, 3, 3, -math.pi / 4, 0.7)
         run_opt_estimator("optzz3x3", q, random_paulis(9, lattice_edges(3), 30, orng), 4, 1e-8, 1e-10, 50, 1e-8)
+    if "tpocount" in jobs:
+        q = kicked_ising_no_barrier(3, 3, 2, -0.6, 0.7)  # 2 x (12 rzz + 9 rx) = 42 instructions
+        run_tpocount("kinb3x3", q, [[21, 21], [10, 15, 17], [5, 30, 40], [42]])
+        crng = np.random.default_rng(20261206)
+        run_count_estimator("kinb3x3", q, random_paulis(9, lattice_edges(3), 30, crng), 4, 1e-8, 1e-10, 50,
+                            [10, 15, 17])
     if "ckpt" in jobs:
         crng = np.random.default_rng(20261205)
         q = kicked_ising_qasm(3, 3, 3, -0.8, 0.6)

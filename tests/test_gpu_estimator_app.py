@@ -101,3 +101,18 @@ def test_estimator_app_measures_cluster_terms():
         want = bn.measure_cluster(edges, V, E, qs, ls)
         assert abs(float(v) - want.real) <= 1e-9, (r, v, want)
     assert "Sum of c_k <P_k> over all terms" in out
+
+
+@pytest.mark.parametrize("precision,tol", [("c128", 1e-9), ("mixed", 1e-6)])
+def test_estimator_app_with_num_gates(precision, tol):
+    """--num_gates (manual gate-number layering, qasmtotpo.h:709-738) on a
+    barrier-free kicked-Ising program split inside its Floquet steps; the
+    fixture holds what the reference app printed with the same flags."""
+    import json
+    ref = json.load(open(os.path.join(HERE, "golden", "count_kinb3x3.json")))
+    one, two, out = _run("kinb3x3", ref, precision, ("--num_gates", ",".join(str(n) for n in ref["num_gates"])))
+    if precision == "c128":
+        assert [int(v) for v in re.findall(r"bond dim = (\d+)", out)] == ref["bond_dims"]
+    assert len(one) == len(ref["one"]) and len(two) == len(ref["two"]), out
+    for a, b in zip(one + two, ref["one"] + ref["two"]):
+        assert abs(a - b) <= tol, (a, b)

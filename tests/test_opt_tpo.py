@@ -173,3 +173,45 @@ def test_abi_errors_and_in_place_repacking():
     assert 0 < nel.value < n_in
     assert off[0] == 0 and np.all(np.diff(off) > 0) and off[-1] < nel.value
     np.testing.assert_array_equal(data[2 * n_in:], guard)
+
+
+def test_manual_gate_number_layering_matches_reference():
+    """QasmToTPO with num_gates (qasmtotpo.h:709-738) against the reference's
+    own overload (tests/golden/tpocount_kinb3x3.npz): layer shapes exact, each
+    layer's full operator within 1e-12 -- splits on step boundaries, inside
+    steps, and with a partly filled last layer."""
+    z = np.load(os.path.join(G, "tpocount_kinb3x3.npz"))
+    edges = [tuple(int(v) for v in e) for e in z["edges"]]
+    src = open(os.path.join(G, "inputs", "kinb3x3.qasm")).read()
+    ns = len(bn.sites_of(edges))
+    k = 0
+    while f"split{k}" in z:
+        split = [int(v) for v in z[f"split{k}"]]
+        layers = tb.QasmToTPOByCount(src, edges, split)
+        nl = 0
+        while f"split{k}/{nl}/0" in z:
+            nl += 1
+        assert len(layers) == nl
+        for l, layer in enumerate(layers):
+            ref = [z[f"split{k}/{l}/{s}"] for s in range(ns)]
+            got = [layer.site_op(edges, s) for s in range(ns)]
+            assert [t.shape for t in got] == [t.shape for t in ref]
+            np.testing.assert_allclose(full_operator(edges, got), full_operator(edges, ref), rtol=0, atol=1e-12)
+        k += 1
+    assert k == 4
+
+
+def test_manual_gate_number_layering_errors():
+    src = open(os.path.join(G, "inputs", "kinb3x3.qasm")).read()
+    edges = tb.EdgesFromQasm(src)
+    for split, code in (([21, 20], tb.EINVAL),        # more instructions than the counts cover
+                        ([21, 21, 5], tb.EINVAL),     # a layer that receives nothing
+                        ([0, 42], tb.EINVAL),         # a count < 1
+                        ([], tb.EINVAL)):
+        with pytest.raises(tb.TnbpError) as e:
+            tb.QasmToTPOByCount(src, edges, split)
+        assert e.value.code == code, split
+    with pytest.raises(tb.TnbpError) as e:  # barriers are gates there: "matrix for this op not implemented"
+        tb.QasmToTPOByCount(open(os.path.join(G, "inputs", "ki3x3.qasm")).read(),
+                            tb.EdgesFromQasm(open(os.path.join(G, "inputs", "ki3x3.qasm")).read()), [500])
+    assert e.value.code == tb.EUNSUPPORTED

@@ -54,6 +54,8 @@ _SIGS = {
     "tnbp_pauli_terms": [C.c_char_p, _i32p, C.c_int64, _i32p, _i32p, _i32p, C.c_char_p, _f64p, _i32p,
                          C.c_int64, _i64p, _i64p],
     "tnbp_qasm_tpo": [C.c_char_p, _i32p, C.c_int64, _i32p, _i64p, _f64p, C.c_int64, _i32p, _i64p],
+    "tnbp_qasm_tpo_counts": [C.c_char_p, _i32p, C.c_int64, _i32p, C.c_int32, _i32p, _i64p, _f64p, C.c_int64, _i32p,
+                             _i64p],
     "tnbp_kicked_ising_tpo": [_i32p, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double, _i32p, _i64p,
                               _f64p, C.c_int64, _i64p],
     "tnbp_opt_tpo_svd": [_i32p, C.c_int64, C.c_double, _i32p, _i64p, _f64p, _i64p],
@@ -287,6 +289,23 @@ def QasmToTPO(src, edges):
     data = np.zeros(2 * max(1, nel.value), np.float64)
     _chk(lib.tnbp_qasm_tpo(s, _p(e, _i32p), len(e), _p(rank, _i32p), _p(off, _i64p), _p(data, _f64p),
                            max(1, nel.value), C.byref(nl), C.byref(nel)))
+    return _layers(len(e), ns, nl.value, rank, off, data.view(np.complex128))
+
+
+def QasmToTPOByCount(src, edges, num_gates):
+    """QasmToTPO with manual gate-number layering (qasmtotpo.h:709-738)."""
+    e = _edges_arr(edges)
+    ns = len(GetSiteIndexFromBond(edges))
+    s = src.encode()
+    ng = np.ascontiguousarray(num_gates, np.int32)
+    nl, nel = C.c_int32(), C.c_int64()
+    _chk(lib.tnbp_qasm_tpo_counts(s, _p(e, _i32p), len(e), _p(ng, _i32p), len(ng), None, None, None, 0,
+                                  C.byref(nl), C.byref(nel)))
+    rank = np.zeros(max(1, nl.value * len(e)), np.int32)
+    off = np.zeros(max(1, nl.value * ns), np.int64)
+    data = np.zeros(2 * max(1, nel.value), np.float64)
+    _chk(lib.tnbp_qasm_tpo_counts(s, _p(e, _i32p), len(e), _p(ng, _i32p), len(ng), _p(rank, _i32p), _p(off, _i64p),
+                                  _p(data, _f64p), max(1, nel.value), C.byref(nl), C.byref(nel)))
     return _layers(len(e), ns, nl.value, rank, off, data.view(np.complex128))
 
 

@@ -7,7 +7,8 @@
 //   --circuit FILE  --sparse_pauli FILE  --max_bond_dim N  --bp_tolerance X
 //   --max_bp_iterations N  --sv_min X  --truncation_error X (accepted, unused
 //   by the reference too)  --backend default  --do_opt_tpo N (nonzero:
-//   OptTPObySVD on every layer)  --eps_opt_tpo X
+//   OptTPObySVD on every layer)  --eps_opt_tpo X  --num_gates n0,n1,...
+//   (manual gate-number layering instead of barriers)
 // plus --precision c128|mixed|c64 (default c128, the drop-in), --sum
 // (print sum_k c_k <P_k>, which the reference does not compute) and
 // --measure_clusters (also measure the terms the reference drops --
@@ -17,8 +18,7 @@
 // condition, the per-edge truncation results and the per-term expectation
 // values (one-site terms first, then two-site terms, each in file order);
 // the reference's time stamps are left out.  Not supported here: the
-// ibm_kobe backend's fixed edge list and --num_gates manual layering, which
-// are outside the BP hot path.
+// ibm_kobe backend's fixed edge list, which is outside the BP hot path.
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -46,6 +46,7 @@ struct Options {
   int max_bp_iterations = 50, max_bond_dim = 100;
   double bp_tolerance = 1.0e-8, sv_min = 1.0e-8, truncation_error = 1.0e-8;
   bool do_opt_tpo = false;
+  std::vector<int> num_gates;
   double eps_opt_tpo = 1.0e-8;
   int precision = TNBP_C128;
   bool print_sum = false;
@@ -79,7 +80,9 @@ Options parse(int argc, char** argv) {
       else if (p == "c64") o.precision = TNBP_C64;
       else throw std::invalid_argument("--precision must be c128, mixed or c64");
     } else if (a == "--num_gates") {
-      throw std::invalid_argument(a + " is not supported by tnbp_estimator");
+      std::stringstream ss(next());
+      std::string tok;
+      while (std::getline(ss, tok, ',')) o.num_gates.push_back(std::stoi(tok));
     }
   }
   if (o.backend != "default") throw std::invalid_argument("only --backend default is supported");
@@ -94,7 +97,8 @@ int run(const Options& o) {
   std::cout << " edges:";
   for (const auto& e : edges) std::cout << " (" << e.first << "," << e.second << ")";
   std::cout << "\n";
-  std::vector<tb::TpoLayer> TPO = tb::QasmToTPO(qasm, edges);
+  std::vector<tb::TpoLayer> TPO =
+      o.num_gates.empty() ? tb::QasmToTPO(qasm, edges) : tb::QasmToTPO(qasm, edges, o.num_gates);
   if (o.do_opt_tpo)
     for (size_t l = 0; l < TPO.size(); ++l) {
       tb::OptTPObySVD(edges, TPO[l], o.eps_opt_tpo);

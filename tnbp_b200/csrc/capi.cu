@@ -181,6 +181,19 @@ int tnbp_qasm_tpo(const char* src, const int32_t* edges, int64_t ne, int32_t* ed
   });
 }
 
+int tnbp_qasm_tpo_counts(const char* src, const int32_t* edges, int64_t ne, const int32_t* num_gates, int32_t n_counts,
+                         int32_t* edge_rank, int64_t* op_offset, double* op_data, int64_t cap, int32_t* n_layers,
+                         int64_t* n_elems) {
+  return guard([&] {
+    need(src != nullptr && (n_counts == 0 || num_gates != nullptr), "NULL argument");
+    auto e = to_edges(edges, ne);
+    auto layers = tnbp_host::qasm_tpo_counts(tnbp_host::parse_qasm(src), e,
+                                             std::vector<int>(num_gates, num_gates + n_counts));
+    if (n_layers) *n_layers = (int32_t)layers.size();
+    put_layers(layers, ne, (int64_t)tnbp_host::site_labels(e).size(), edge_rank, op_offset, op_data, cap, n_elems);
+  });
+}
+
 int tnbp_kicked_ising_tpo(const int32_t* edges, int64_t ne, double Jz, double hz, double hx, double dt,
                           int32_t* edge_rank, int64_t* op_offset, double* op_data, int64_t cap, int64_t* n_elems) {
   return guard([&] {

@@ -862,6 +862,40 @@ std::vector<Layer> qasm_tpo(const Program& p, const Edges& edges) {
   return out;
 }
 
+// QasmToTPO with manual gate-number layering (qasmtotpo.h:709-738): layer m
+// takes the next num_gates[m] instructions.  Every instruction is appended as
+// a gate, so a barrier (like measure / reset / custom) is an unsupported
+// operation there.  The reference writes past its layer vector when the
+// program has more instructions than the counts cover and leaves a layer
+// that receives no instruction uninitialized; both are refused here.
+std::vector<Layer> qasm_tpo_counts(const Program& p, const Edges& edges, const std::vector<int>& num_gates) {
+  if (num_gates.empty()) throw HostError(-1, "num_gates is empty");
+  for (int n : num_gates)
+    if (n < 1) throw HostError(-1, "num_gates entries must be >= 1");
+  long long total = 0;
+  for (int n : num_gates) total += n;
+  if ((long long)p.instructions.size() > total)
+    throw HostError(-1, "the program has more instructions than num_gates covers");
+  LayerBuilder lb(edges);
+  std::vector<Layer> out;
+  int count = 0;
+  size_t m = 0;
+  for (const auto& in : p.instructions) {
+    if (in.op == Op::BARRIER || in.op == Op::MEASURE || in.op == Op::RESET || in.op == Op::CUSTOM)
+      throw HostError(-6, "matrix for this op not implemented");
+    lb.append(in);
+    if (++count == num_gates[m]) {
+      out.push_back(pack_layer(lb));
+      lb.reset();
+      count = 0;
+      ++m;
+    }
+  }
+  if (count > 0) { out.push_back(pack_layer(lb)); ++m; }
+  if (m != num_gates.size()) throw HostError(-1, "a layer of num_gates receives no instruction");
+  return out;
+}
+
 // One Floquet step of apps/kicked_ising_lattice/circuit.h:14-229:
 // exp(-i dt Jz Z Z) on every edge, then exp(-i dt hz Z), then exp(-i dt hx X).
 // exp(-i th ZZ) = cos(th) I(x)I - i sin(th) Z(x)Z, split term by term with

@@ -56,6 +56,7 @@ Program parse_qasm(const std::string& src);
 int qubit_count(const Instruction& in);
 Edges qasm_edges(const Program& p);
 std::vector<Layer> qasm_tpo(const Program& p, const Edges& edges);
+std::vector<Layer> qasm_tpo_counts(const Program& p, const Edges& edges, const std::vector<int>& num_gates);
 Layer kicked_ising_tpo(const Edges& edges, double Jz, double hz, double hx, double dt);
 void opt_tpo_svd(const Edges& edges, Layer& layer, double eps);
 std::vector<PauliTerm> pauli_terms(const std::string& text, const Edges& edges, int64_t* n_dropped);
