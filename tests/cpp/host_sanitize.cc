@@ -1,4 +1,4 @@
-// The engine's host code (tnbp_b200/csrc/host_setup.cpp, tps_io.cpp) under
+// The engine's host code (tnbp_b200/csrc/host_setup.cpp, qasm_text.cpp, tps_io.cpp) under
 // AddressSanitizer / UndefinedBehaviorSanitizer: every golden QASM program,
 // observable and checkpoint, then seeded truncations and byte mutations of
 // them.  Malformed input must end in a HostError (a status code at the C

@@ -29,7 +29,7 @@ oracle/_ref/, and this script runs them on seeded synthetic inputs:
   config1.json       observables of the 4x4 kicked-Ising workload from the
                      reference apps kicked_ising_lattice and estimator
 
-usage: python tests/golden/make_golden.py [--ref /root/reference]
+usage: python tests/golden/make_golden.py [--ref <reference tree>]   (default: $TNBP_REFERENCE)
 Needs the reference sources (only in the build container); the fixtures it
 writes are what the tests read everywhere else.
 """
@@ -47,6 +47,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, HERE)
 from records import read_records  # noqa: E402
+
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+from reference_root import reference_root  # noqa: E402
 
 INPUTS = os.path.join(HERE, "inputs")
 REF_BIN = os.path.join(ROOT, "oracle", "_ref")
@@ -372,7 +375,7 @@ def run_config1():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=reference_root())
     ap.add_argument("--only", default="")
     a = ap.parse_args()
     subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), f"REF={a.ref}"])

@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 import bp_numpy as bn
+from reference_root import reference_file, reference_root
 
 tb = pytest.importorskip("tnbp_b200")
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -38,10 +39,10 @@ def test_host_builders_bit_exact(path):
         _graph_checks(tb.bond_square_lattice(Lx, Ly), ref)
         return
     if name in ("kobe", "ising_circuit"):
-        pytest.skip("input lives in the reference tree") if not os.path.exists("/root/reference") else None
-        base = "/root/reference/apps/" + ("estimator/kicked_ising.qasm" if name == "kobe" else "qasm_tpo/ising_circuit.qasm")
+        pytest.skip("input lives in the reference tree") if not os.path.exists(reference_root()) else None
+        base = reference_file("apps", "estimator/kicked_ising.qasm" if name == "kobe" else "qasm_tpo/ising_circuit.qasm")
         src = open(base).read()
-        ptxt = open("/root/reference/apps/estimator/H_ising_kobe.txt").read() if name == "kobe" else None
+        ptxt = open(reference_file("apps", "estimator", "H_ising_kobe.txt")).read() if name == "kobe" else None
     else:
         src = open(os.path.join(G, "inputs", f"{name}.qasm")).read()
         pp = os.path.join(G, "inputs", f"{name}.txt")

@@ -20,7 +20,8 @@ def test_host_code_under_asan_ubsan(tmp_path):
     exe = str(tmp_path / "host_sanitize")
     subprocess.run(["g++", "-std=c++17", "-O1", "-g", "-fsanitize=address,undefined", "-fno-sanitize-recover=all",
                     "-fno-omit-frame-pointer", "-I", CSRC, os.path.join(ROOT, "tests", "cpp", "host_sanitize.cc"),
-                    os.path.join(CSRC, "host_setup.cpp"), os.path.join(CSRC, "tps_io.cpp"), "-o", exe], check=True)
+                    os.path.join(CSRC, "host_setup.cpp"),
+                    os.path.join(CSRC, "qasm_text.cpp"), os.path.join(CSRC, "tps_io.cpp"), "-o", exe], check=True)
     qasm = sorted(glob.glob(os.path.join(G, "inputs", "*.qasm")))
     pauli = sorted(glob.glob(os.path.join(G, "inputs", "*.txt")))
     ckpt = [os.path.join(G, "ckpt_ki3x3r000000.dat"), os.path.join(G, "inputs", "ki3x3r.qasm")]

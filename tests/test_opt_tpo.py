@@ -17,11 +17,12 @@ import numpy as np
 import pytest
 
 import bp_numpy as bn
+from reference_root import reference_file, reference_root
 
 tb = pytest.importorskip("tnbp_b200")
 HERE = os.path.dirname(os.path.abspath(__file__))
 G = os.path.join(HERE, "golden")
-KOBE = "/root/reference/apps/estimator/kicked_ising.qasm"
+KOBE = reference_file("apps", "estimator", "kicked_ising.qasm")
 SMALL = [("zzcx3x3", "eps1e-08"), ("zzcx3x3", "eps1000"), ("optmix2x3", "eps1e-08")]
 
 

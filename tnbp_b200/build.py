@@ -17,7 +17,7 @@ APP = os.path.join(HERE, "tnbp_estimator")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["engine.cu", "capi.cu", "server.cu", "noalloc.cu", "host_setup.cpp", "tps_io.cpp", "trace.cpp"]
+SOURCES = ["engine.cu", "capi.cu", "server.cu", "noalloc.cu", "host_setup.cpp", "qasm_text.cpp", "tps_io.cpp", "trace.cpp"]
 
 
 def _headers():

@@ -110,413 +110,13 @@ std::vector<int> shortest_path(const Edges& e, int src, int dst) {
   return path;
 }
 
-// ---------------------------------------------------------------- QASM
-// Grammar and broadcasting of include/qasm/{common/reader,v2/parser,
-// v3/parser}.h: expressions with + - * / ( ) unary sign, pi and tau, numbers
-// via strtod; a register argument expands to all its qubits; a gate whose
-// argument count is a multiple of its arity is split into consecutive
-// groups; barrier keeps all its qubits in one instruction.
-namespace {
-struct Reader {
-  std::string src;
-  size_t i = 0, line = 1, col = 1;
-  bool eof() const { return i >= src.size(); }
-  char peek() const { return eof() ? '\0' : src[i]; }
-  char get() {
-    if (eof()) return '\0';
-    char c = src[i++];
-    if (c == '\n') { ++line; col = 1; } else ++col;
-    return c;
-  }
-  [[noreturn]] void err(const std::string& m) const {
-    throw HostError(-5, "QASM parse error (" + std::to_string(line) + ":" + std::to_string(col) + "): " + m);
-  }
-  static bool id0(char c) { return std::isalpha((unsigned char)c) || c == '_'; }
-  static bool id1(char c) { return std::isalnum((unsigned char)c) || c == '_' || c == '$'; }
-  void ws() {
-    for (;;) {
-      while (!eof() && std::isspace((unsigned char)peek())) get();
-      if (peek() == '/' && i + 1 < src.size() && src[i + 1] == '/') { while (!eof() && get() != '\n') {} continue; }
-      if (peek() == '/' && i + 1 < src.size() && src[i + 1] == '*') {
-        get(); get();
-        while (!eof()) { char c = get(); if (c == '*' && peek() == '/') { get(); break; } }
-        continue;
-      }
-      break;
-    }
-  }
-  std::string word() {
-    ws();
-    if (!id0(peek())) err("identifier expected");
-    std::string w(1, get());
-    while (id1(peek())) w.push_back(get());
-    return w;
-  }
-  static bool ieq(const std::string& a, const char* b) {
-    size_t n = std::strlen(b);
-    if (a.size() != n) return false;
-    for (size_t k = 0; k < n; ++k)
-      if (std::tolower((unsigned char)a[k]) != std::tolower((unsigned char)b[k])) return false;
-    return true;
-  }
-  bool peek_word(const char* w) {
-    ws();
-    if (!id0(peek())) return false;
-    size_t si = i, sl = line, sc = col;
-    std::string t = word();
-    i = si; line = sl; col = sc;
-    return ieq(t, w);
-  }
-  void expect(char ch) {
-    ws();
-    if (peek() != ch) err(std::string("expected '") + ch + "'");
-    get();
-  }
-  void version() {
-    ws();
-    if (peek() == '"') { get(); while (!eof() && get() != '"') {} return; }
-    while (!eof() && (std::isdigit((unsigned char)peek()) || peek() == '.')) get();
-  }
-  double number() {
-    ws();
-    size_t s = i;
-    bool dot = false, ex = false;
-    if (peek() == '+' || peek() == '-') get();
-    while (!eof()) {
-      char c = peek();
-      if (std::isdigit((unsigned char)c)) get();
-      else if (c == '.' && !dot) { dot = true; get(); }
-      else if ((c == 'e' || c == 'E') && !ex) { ex = true; get(); if (peek() == '+' || peek() == '-') get(); }
-      else break;
-    }
-    if (i == s) err("number expected");
-    return std::strtod(src.substr(s, i - s).c_str(), nullptr);
-  }
-  double factor() {
-    ws();
-    char c = peek();
-    if (c == '(') { get(); double v = expr(); expect(')'); return v; }
-    if (c == '+' || c == '-') { bool neg = c == '-'; get(); double v = factor(); return neg ? -v : v; }
-    if (id0(c)) {
-      std::string w = word();
-      if (ieq(w, "pi")) return 3.14159265358979323846;
-      if (ieq(w, "tau")) return 6.28318530717958647692;
-      err("unknown symbol in expression: " + w);
-    }
-    return number();
-  }
-  double term() {
-    double v = factor();
-    for (;;) {
-      ws();
-      char c = peek();
-      if (c == '*') { get(); v *= factor(); }
-      else if (c == '/') { get(); double d = factor(); if (d == 0.0) err("division by zero"); v /= d; }
-      else break;
-    }
-    return v;
-  }
-  double expr() {
-    double v = term();
-    for (;;) {
-      ws();
-      char c = peek();
-      if (c == '+') { get(); v += term(); }
-      else if (c == '-') { get(); v -= term(); }
-      else break;
-    }
-    return v;
-  }
-  std::vector<double> params() {
-    std::vector<double> p;
-    expect('(');
-    ws();
-    if (peek() != ')') {
-      for (;;) { p.push_back(expr()); ws(); if (peek() == ',') { get(); continue; } break; }
-    }
-    expect(')');
-    return p;
-  }
-};
-
-Op map_gate(const std::string& g) {
-  auto L = [&](const char* s) { return Reader::ieq(g, s); };
-  if (L("u3") || L("u")) return Op::U3;
-  if (L("u2")) return Op::U2;
-  if (L("u1") || L("p")) return Op::U1;
-  if (L("rx")) return Op::RX;
-  if (L("ry")) return Op::RY;
-  if (L("rz")) return Op::RZ;
-  if (L("h")) return Op::H;
-  if (L("x")) return Op::X;
-  if (L("y")) return Op::Y;
-  if (L("z")) return Op::Z;
-  if (L("s")) return Op::S;
-  if (L("sdg")) return Op::SDG;
-  if (L("t")) return Op::T;
-  if (L("tdg")) return Op::TDG;
-  if (L("id")) return Op::ID;
-  if (L("cx") || L("cnot")) return Op::CX;
-  if (L("cz")) return Op::CZ;
-  if (L("swap")) return Op::SWAP;
-  if (L("rzz")) return Op::RZZ;
-  if (L("ccx") || L("toffoli")) return Op::CCX;
-  if (L("cswap")) return Op::CSWAP;
-  return Op::CUSTOM;
-}
-size_t arity(Op op) {
-  switch (op) {
-    case Op::U3: case Op::U2: case Op::U1: case Op::RX: case Op::RY: case Op::RZ: case Op::H:
-    case Op::X: case Op::Y: case Op::Z: case Op::S: case Op::SDG: case Op::T: case Op::TDG: case Op::ID:
-      return 1;
-    case Op::CX: case Op::CZ: case Op::SWAP: case Op::RZZ: return 2;
-    case Op::CCX: case Op::CSWAP: return 3;
-    default: return 0;
-  }
-}
-
-struct Parser {
-  Reader r;
-  bool v3 = false;
-  Program prog;
-  std::unordered_map<std::string, size_t> qsz, csz;
-
-  void check_q(const std::string& reg, size_t idx) {
-    auto it = qsz.find(reg);
-    if (it == qsz.end()) r.err("unknown qreg: " + reg);
-    if (idx >= it->second) r.err("qreg index out of range: " + reg + "[" + std::to_string(idx) + "]");
-  }
-  void check_c(const std::string& reg, size_t idx) {
-    auto it = csz.find(reg);
-    if (it == csz.end()) r.err("unknown creg: " + reg);
-    if (idx >= it->second) r.err("creg index out of range: " + reg + "[" + std::to_string(idx) + "]");
-  }
-  std::vector<QArg> one_qarg() {
-    r.ws();
-    std::string reg = r.word();
-    r.ws();
-    if (r.peek() == '[') {
-      r.get();
-      r.ws();
-      size_t lo = (size_t)r.number();
-      r.ws();
-      if (v3 && r.peek() == ':') {
-        r.get();
-        r.ws();
-        size_t hi = (size_t)r.number();
-        r.expect(']');
-        auto it = qsz.find(reg);
-        if (it == qsz.end()) r.err("unknown qreg: " + reg);
-        if (hi < lo || hi > it->second) r.err("slice out of range");
-        std::vector<QArg> v;
-        for (size_t k = lo; k < hi; ++k) v.push_back({reg, k});
-        return v;
-      }
-      r.expect(']');
-      check_q(reg, lo);
-      return {{reg, lo}};
-    }
-    auto it = qsz.find(reg);
-    if (it == qsz.end()) r.err("unknown qreg: " + reg);
-    std::vector<QArg> v;
-    for (size_t k = 0; k < it->second; ++k) v.push_back({reg, k});
-    return v;
-  }
-  std::vector<QArg> qargs(bool many) {
-    auto out = one_qarg();
-    if (!many) return out;
-    r.ws();
-    while (r.peek() == ',') {
-      r.get();
-      auto nx = one_qarg();
-      out.insert(out.end(), nx.begin(), nx.end());
-      r.ws();
-    }
-    return out;
-  }
-  void push(Op op, std::vector<QArg> q, std::vector<double> p) {
-    Instruction in;
-    in.op = op;
-    in.qubits = std::move(q);
-    in.params = std::move(p);
-    prog.instructions.push_back(std::move(in));
-  }
-  void include() { r.word(); r.ws(); r.expect('"'); while (!r.eof() && r.get() != '"') {} r.expect(';'); }
-  void reg_decl(bool quantum) {  // v2: qreg/creg name[n];
-    r.word();
-    std::string nm = r.word();
-    r.ws();
-    r.expect('[');
-    size_t n = (size_t)r.number();
-    r.expect(']');
-    r.expect(';');
-    (quantum ? qsz : csz)[nm] = n;
-  }
-  void decl_v3(bool quantum) {  // v3: qubit[n] name; / bit[n] name;
-    r.word();
-    r.ws();
-    size_t n = 1;
-    if (r.peek() == '[') { r.get(); n = (size_t)r.number(); r.expect(']'); }
-    std::string nm = r.word();
-    r.expect(';');
-    (quantum ? qsz : csz)[nm] = n;
-  }
-  void barrier() { r.word(); auto q = qargs(true); r.expect(';'); push(Op::BARRIER, q, {}); }
-  void reset() {
-    r.word();
-    auto q = qargs(true);
-    r.expect(';');
-    for (auto& a : q) push(Op::RESET, {a}, {});
-  }
-  std::pair<std::string, size_t> carg() {
-    r.ws();
-    std::string reg = r.word();
-    r.ws();
-    if (v3 && r.peek() != '[') {
-      auto it = csz.find(reg);
-      if (it == csz.end()) r.err("unknown bit/creg: " + reg);
-      if (it->second != 1) r.err("missing index for creg: " + reg);
-      return {reg, 0};
-    }
-    r.expect('[');
-    size_t idx = (size_t)r.number();
-    r.expect(']');
-    check_c(reg, idx);
-    return {reg, idx};
-  }
-  void measure_arrow() {
-    r.word();
-    auto q = qargs(false);
-    r.ws();
-    if (!(r.peek() == '-' && r.i + 1 < r.src.size() && r.src[r.i + 1] == '>')) r.err("expected '->' after measure");
-    r.get(); r.get();
-    carg();
-    r.expect(';');
-    if (q.size() != 1) r.err("measure expects a single qubit");
-    push(Op::MEASURE, {q[0]}, {});
-  }
-  bool looks_bit_assign() {
-    size_t si = r.i, sl = r.line, sc = r.col;
-    r.ws();
-    bool ok = false;
-    if (r.peek_word("bit")) {
-      r.word();
-      r.ws();
-      if (Reader::id0(r.peek())) { r.word(); r.ws(); ok = r.peek() == '='; }
-    }
-    r.i = si; r.line = sl; r.col = sc;
-    return ok;
-  }
-  bool looks_creg_assign() {
-    size_t si = r.i, sl = r.line, sc = r.col;
-    r.ws();
-    bool ok = false;
-    if (Reader::id0(r.peek())) {
-      r.word();
-      r.ws();
-      if (r.peek() == '[') { r.get(); r.number(); r.expect(']'); }
-      r.ws();
-      ok = r.peek() == '=';
-    }
-    r.i = si; r.line = sl; r.col = sc;
-    return ok;
-  }
-  void measure_assign() {
-    r.ws();
-    if (r.peek_word("bit")) {
-      r.word();
-      r.ws();
-      if (r.peek() == '[') r.err("bit array not allowed on LHS with declaration here");
-      std::string nm = r.word();
-      if (!csz.count(nm)) csz[nm] = 1;
-    } else {
-      carg();
-    }
-    r.ws();
-    r.expect('=');
-    r.ws();
-    if (!r.peek_word("measure")) r.err("expected 'measure' in assignment");
-    r.word();
-    auto q = qargs(false);
-    r.expect(';');
-    if (q.size() != 1) r.err("measure expects a single qubit");
-    push(Op::MEASURE, {q[0]}, {});
-  }
-  void gate() {
-    std::string g = r.word();
-    if (v3 && (Reader::ieq(g, "ctrl") || Reader::ieq(g, "inv") || Reader::ieq(g, "pow")))
-      r.err("gate modifiers are not supported in this subset");
-    std::vector<double> p;
-    r.ws();
-    if (r.peek() == '(') p = r.params();
-    r.ws();
-    auto q = qargs(true);
-    r.expect(';');
-    const Op op = map_gate(g);
-    const size_t ar = arity(op);
-    if (ar > 0 && q.size() % ar != 0) r.err("gate '" + g + "' expects multiple of " + std::to_string(ar) + " qubits");
-    if (ar == 0) { push(op, q, p); return; }
-    for (size_t k = 0; k < q.size(); k += ar)
-      push(op, std::vector<QArg>(q.begin() + k, q.begin() + k + ar), p);
-  }
-  Program parse(const std::string& s, bool version3) {
-    r.src = s;
-    v3 = version3;
-    r.ws();
-    if (v3) {
-      if (!r.peek_word("OPENQASM")) r.err("OPENQASM header required for v3");
-      r.word(); r.version(); r.expect(';');
-    } else if (r.peek_word("OPENQASM")) {
-      r.word(); r.version(); r.expect(';');
-    }
-    while (!r.eof()) {
-      r.ws();
-      if (r.eof()) break;
-      if (r.peek_word("include")) { include(); continue; }
-      if (!v3) {
-        if (r.peek_word("qreg")) { reg_decl(true); continue; }
-        if (r.peek_word("creg")) { reg_decl(false); continue; }
-        if (r.peek_word("barrier")) { barrier(); continue; }
-        if (r.peek_word("reset")) { reset(); continue; }
-        if (r.peek_word("measure")) { measure_arrow(); continue; }
-        gate();
-        continue;
-      }
-      if (r.peek_word("qubit")) { decl_v3(true); continue; }
-      if (r.peek_word("barrier")) { barrier(); continue; }
-      if (r.peek_word("reset")) { reset(); continue; }
-      if (r.peek_word("measure")) { measure_arrow(); continue; }
-      if (looks_bit_assign() || looks_creg_assign()) { measure_assign(); continue; }
-      if (r.peek_word("bit")) { decl_v3(false); continue; }
-      {
-        size_t si = r.i, sl = r.line, sc = r.col;
-        std::string w = r.word();
-        if (Reader::ieq(w, "ctrl") || Reader::ieq(w, "inv") || Reader::ieq(w, "pow"))
-          r.err("gate modifiers (ctrl/inv/pow) are not supported in this subset");
-        r.i = si; r.line = sl; r.col = sc;
-      }
-      gate();
-    }
-    return prog;
-  }
-};
-}  // namespace
-
-// parse_any (include/qasm/any.h:8-21): v3 when the 32 characters after
-// "OPENQASM" contain a '3', else v2.
-Program parse_qasm(const std::string& src) {
-  const auto pos = src.find("OPENQASM");
-  bool is3 = false;
-  if (pos != std::string::npos) is3 = src.substr(pos, 32).find('3') != std::string::npos;
-  Parser p;
-  return p.parse(src, is3);
-}
+// QASM text: qasm_text.cpp (tokenizer and statement reader).
 
 int qubit_count(const Instruction& in) {
   switch (in.op) {
     case Op::MEASURE: case Op::RESET: return 1;
     case Op::BARRIER: case Op::CUSTOM: return (int)in.qubits.size();
-    default: return (int)arity(in.op);
+    default: return op_arity(in.op);
   }
 }
 
@@ -1057,21 +657,9 @@ void opt_tpo_svd(const Edges& edges, Layer& layer, double eps) {
 }
 
 // -------------------------------------------------------------- Pauli
-// load_sparse_pauli_op (sparse_pauli.h:52-97) on text; classification of
-// ClassifyOps (paulitotpo.h:99-153).
-static void trim(std::string& s) {
-  auto ns = [](unsigned char c) { return !std::isspace(c); };
-  auto b = std::find_if(s.begin(), s.end(), ns);
-  auto e = std::find_if(s.rbegin(), s.rend(), ns).base();
-  if (b < e) s.assign(b, e); else s.clear();
-}
-
+// Rows of the observable text come from pauli_rows (qasm_text.cpp);
+// classification of ClassifyOps (paulitotpo.h:99-153).
 namespace {
-struct PauliRow {
-  double re = 0, im = 0;
-  std::vector<std::pair<int, char>> ops;  // non-identity letters, ascending qubit
-};
-
 bool adjacent(const Edges& edges, int a, int b) {
   for (int m : surrounding_bonds(edges, a)) {
     const auto& e = edges[m];
@@ -1080,42 +668,6 @@ bool adjacent(const Edges& edges, int a, int b) {
   return false;
 }
 
-std::vector<PauliRow> pauli_rows(const std::string& text) {
-  std::vector<PauliRow> rows;
-  std::istringstream in(text);
-  std::string line;
-  size_t lineno = 0;
-  while (std::getline(in, line)) {
-    ++lineno;
-    trim(line);
-    if (line.empty() || line.rfind("#", 0) == 0 || line.rfind("//", 0) == 0) continue;
-    double re = 0, im = 0;
-    std::string ps;
-    std::istringstream a(line);
-    if (!(a >> re >> im >> ps)) {
-      std::istringstream b(line);
-      im = 0;
-      if (!(b >> re >> ps)) throw HostError(-5, "Parse error at line " + std::to_string(lineno) + ": \"" + line + "\"");
-    }
-    trim(ps);
-    for (char& ch : ps) {
-      ch = (char)std::toupper((unsigned char)ch);
-      if (ch != 'I' && ch != 'X' && ch != 'Y' && ch != 'Z')
-        throw HostError(-5, "Invalid Pauli label: only I/X/Y/Z are allowed.");
-    }
-    // rightmost character is qubit 0; keep non-identity letters, ascending qubit
-    PauliRow r;
-    r.re = re;
-    r.im = im;
-    const size_t n = ps.size();
-    for (size_t i = 0; i < n; ++i) {
-      const char u = ps[n - 1 - i];
-      if (u != 'I') r.ops.push_back({(int)i, u});
-    }
-    rows.push_back(std::move(r));
-  }
-  return rows;
-}
 }  // namespace
 
 std::vector<PauliTerm> pauli_terms(const std::string& text, const Edges& edges, int64_t* n_dropped) {

@@ -52,7 +52,16 @@ std::vector<int> greedy_layering(const Edges& e, int* nlayers);
 std::vector<int> surrounding_bonds(const Edges& e, int site);
 std::vector<int> site_labels(const Edges& e);
 std::vector<int> shortest_path(const Edges& e, int src, int dst);
-Program parse_qasm(const std::string& src);
+// One parsed line of a sparse-Pauli text: coefficient and the non-identity
+// letters with their qubits (ascending; the rightmost letter is qubit 0).
+struct PauliRow {
+  double re = 0, im = 0;
+  std::vector<std::pair<int, char>> ops;
+};
+
+Program parse_qasm(const std::string& src);          // qasm_text.cpp
+int op_arity(Op op);                                 // qasm_text.cpp
+std::vector<PauliRow> pauli_rows(const std::string& text);  // qasm_text.cpp
 int qubit_count(const Instruction& in);
 Edges qasm_edges(const Program& p);
 std::vector<Layer> qasm_tpo(const Program& p, const Edges& edges);
