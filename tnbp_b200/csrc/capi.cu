@@ -316,12 +316,34 @@ int tnbp_load_state(tnbp_job* job, const char* path) {
     std::vector<int> bd, pd;
     tnbp_host::tps_check_whole(st, J.g.edges, bd, pd);
     need(pd == J.pd, "checkpoint physical dimensions differ from the job's");
+    // New layout and buffers are built beside the job's own and swapped in
+    // only after every check and allocation succeeded, so a refused or
+    // failed load leaves the job's state as it was.
+    const std::vector<int> old_dim = J.dim;
+    const std::vector<size_t> old_voff = J.voff, old_moff = J.moff;
+    const size_t old_v = J.v_elems, old_m = J.m_elems;
     J.dim = bd;
     J.layout();
-    J.V.alloc(J.v_elems * J.esz, J.stream);
-    J.M[0].alloc(J.m_elems * J.esz, J.stream);
-    J.M[1].alloc(J.m_elems * J.esz, J.stream);
-    J.check_budget();
+    auto restore = [&] {
+      J.dim = old_dim; J.voff = old_voff; J.moff = old_moff; J.v_elems = old_v; J.m_elems = old_m;
+    };
+    tnbp::DevBuf nV, nM0, nM1;
+    try {
+      const uint64_t extra = (uint64_t)(J.v_elems + 2 * J.m_elems) * J.esz;
+      const uint64_t held = J.V.bytes + J.M[0].bytes + J.M[1].bytes;
+      if (J.budget && J.device_bytes() - held + extra > J.budget)
+        throw tnbp::Error(TNBP_ENOMEM, "checkpoint needs " + std::to_string(J.device_bytes() - held + extra) +
+                                           " device bytes, budget " + std::to_string(J.budget));
+      nV.alloc(J.v_elems * J.esz, J.stream);
+      nM0.alloc(J.m_elems * J.esz, J.stream);
+      nM1.alloc(J.m_elems * J.esz, J.stream);
+    } catch (...) {
+      restore();
+      throw;
+    }
+    std::swap(J.V, nV);
+    std::swap(J.M[0], nM0);
+    std::swap(J.M[1], nM1);
     std::vector<double> hv(2 * J.v_elems, 0.0), hm(2 * J.m_elems, 0.0);
     for (size_t s = 0; s < st.V.size(); ++s)
       std::memcpy(hv.data() + 2 * J.voff[s], st.V[s].data.data(), st.V[s].data.size() * 16);

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 #include <string>
@@ -43,6 +44,24 @@ void check_cuda(cudaError_t e, const char* what, const char* file, int line) {
     throw Error(TNBP_ECUDA, std::string(what) + ": " + cudaGetErrorString(e) + " (" + file + ":" +
                                 std::to_string(line) + ")");
   }
+}
+
+// Per-device one-time settings (the memory pool's release threshold, the
+// opt-in dynamic shared memory of the sweep kernels) belong to a device
+// context: each kernel family records, per
+// device ordinal, that they were set, under one mutex, so several devices
+// and threads may share the library.
+static std::mutex g_attr_mu;
+static bool attr_done(std::vector<char>& flags) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if ((int)flags.size() <= dev) flags.resize(dev + 1, 0);
+  return flags[dev] != 0;
+}
+static void attr_mark(std::vector<char>& flags) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  flags[dev] = 1;
 }
 
 // ----------------------------------------------------------------- memory
@@ -81,15 +100,16 @@ static inline size_t align_elems(size_t n) { return (n + 31) & ~size_t(31); }
 // returning it to the driver each time (the default threshold of 0 makes
 // every large re-allocation map fresh pages).
 void keep_pool_memory() {
-  static bool done = false;
-  if (done) return;
+  static std::vector<char> flags;
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  if (attr_done(flags)) return;
   int dev = 0;
   CK(cudaGetDevice(&dev));
   cudaMemPool_t pool;
   CK(cudaDeviceGetDefaultMemPool(&pool, dev));
   uint64_t thr = UINT64_MAX;
   CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
-  done = true;
+  attr_mark(flags);
 }
 
 // ------------------------------------------------------------------ graph
@@ -628,14 +648,14 @@ static size_t leg_smem(int max_din) {
   return (size_t)(kRowTile * (max_din + 1) + max_din * (kColTile + 1)) * sizeof(typename cvec<R>::type);
 }
 
-// Largest dynamic shared memory any leg-apply launch may ask for; set once
-// per process outside of stream capture.
+// Largest dynamic shared memory any leg-apply launch may ask for.
 template <typename R, typename MR>
 static void leg_apply_attr() {
-  static bool done = false;
-  if (done) return;
+  static std::vector<char> flags;
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  if (attr_done(flags)) return;
   CK(cudaFuncSetAttribute(k_leg_apply<R, MR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)leg_smem<R>(128)));
-  done = true;
+  attr_mark(flags);
 }
 
 template <typename R, typename MR>
@@ -718,22 +738,22 @@ int launch_batch(const SweepBatch& b, int prec, cudaStream_t stream) {
 
 template <typename MR>
 static void tc_attr() {
-  static bool done = false;
-  if (done) return;
+  static std::vector<char> flags, gram_flags;
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  if (attr_done(flags)) return;
   CK(cudaFuncSetAttribute(k_leg_apply_tc<MR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)tc::leg_smem_bytes()));
   CK(cudaFuncSetAttribute(k_leg_apply_tc_bulk<MR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)tc::bulk_smem_bytes()));
   CK(cudaFuncSetAttribute(k_leg_apply_tc64<MR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)tc::leg64_smem_bytes()));
-  static bool gram_done = false;
-  if (!gram_done) {
+  if (!attr_done(gram_flags)) {
     CK(cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::gram_smem_bytes()));
     CK(cudaFuncSetAttribute(k_gram_tc64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)tc::gram64_smem_bytes()));
-    gram_done = true;
+    attr_mark(gram_flags);
   }
-  done = true;
+  attr_mark(flags);
 }
 
 void prepare_kernels(int prec) {
@@ -749,13 +769,13 @@ void prepare_kernels(int prec) {
 }
 
 int num_sms() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
-    CK(cudaGetDevice(&dev));
-    CK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
-  }
-  return n;
+  static std::vector<int> per_dev;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  if ((int)per_dev.size() <= dev) per_dev.resize(dev + 1, 0);
+  if (!per_dev[dev]) CK(cudaDeviceGetAttribute(&per_dev[dev], cudaDevAttrMultiProcessorCount, dev));
+  return per_dev[dev];
 }
 
 // The tcgen05 leg kernel serves complex64 levels with dims <= 32; setting

@@ -62,6 +62,23 @@ unsigned char* scratch_for_current_device() {
   return static_cast<unsigned char*>(g_scratch_ptr[dev]);
 }
 
+// Every descriptor of one call, stored at the start of the scratch array.
+struct NoallocTasks {
+  long long zero;  // the one-entry block-prefix array of every launch
+  int nleg;
+  LegTask leg[kMaxLegs];
+  GramTask gram;
+  MsgTask msg;
+};
+
+// Copies the by-value parameter block into device memory (word by word).
+__global__ void k_store_noalloc_tasks(const NoallocTasks pack, NoallocTasks* dst) {
+  static_assert(sizeof(NoallocTasks) % sizeof(unsigned int) == 0, "word copy");
+  const unsigned int* src = reinterpret_cast<const unsigned int*>(&pack);
+  unsigned int* out = reinterpret_cast<unsigned int*>(dst);
+  for (size_t i = threadIdx.x; i < sizeof(NoallocTasks) / sizeof(unsigned int); i += blockDim.x) out[i] = src[i];
+}
+
 void message_noalloc(const double* site, const int32_t* shape, int32_t rank, int32_t target,
                      const double* const* msgs, double* out, cudaStream_t stream) {
   if (!site || !shape || !msgs || !out) throw Error(TNBP_EINVAL, "NULL argument");
@@ -131,29 +148,30 @@ void message_noalloc(const double* site, const int32_t* shape, int32_t rank, int
   mt.dist = nullptr;
   mt.norm_out = nullptr;
 
-  // task descriptors into the scratch array (H2D copies allocate nothing)
-  size_t off = 0;
-  auto put = [&](const void* p, size_t bytes) -> void* {
-    off = (off + 255) & ~size_t(255);
-    if (off + bytes > kTaskBytes) throw Error(TNBP_EINVAL, "task area of the no-allocation scratch exceeded");
-    void* dst = tasks_area + off;
-    CK(cudaMemcpyAsync(dst, p, bytes, cudaMemcpyHostToDevice, stream));
-    off += bytes;
-    return dst;
-  };
-  const long long zero = 0;
-  const long long* d_zero = static_cast<const long long*>(put(&zero, sizeof(zero)));
-  std::vector<const LegTask*> d_legs;
-  for (auto& t : legs) d_legs.push_back(static_cast<const LegTask*>(put(&t, sizeof(t))));
-  const GramTask* d_gram = static_cast<const GramTask*>(put(&gt, sizeof(gt)));
-  const MsgTask* d_msg = static_cast<const MsgTask*>(put(&mt, sizeof(mt)));
+  // Task descriptors: passed BY VALUE as the parameter block of one small
+  // kernel that stores them into the scratch array, so nothing is read from
+  // host memory after this call returns (a pageable host copy would not be
+  // stream-ordered like the kernels that read the descriptors).
+  NoallocTasks pack{};
+  pack.nleg = (int)legs.size();
+  for (size_t i = 0; i < legs.size(); ++i) pack.leg[i] = legs[i];
+  pack.gram = gt;
+  pack.msg = mt;
+  NoallocTasks* d_pack = reinterpret_cast<NoallocTasks*>(tasks_area);
+  static_assert(sizeof(NoallocTasks) <= kTaskBytes, "task area too small");
+  k_store_noalloc_tasks<<<1, 128, 0, stream>>>(pack, d_pack);
+  CK(cudaGetLastError());
+  note_launch(1);
+  const long long* d_zero = &d_pack->zero;
+  const GramTask* d_gram = &d_pack->gram;
+  const MsgTask* d_msg = &d_pack->msg;
 
   prepare_kernels(TNBP_C128);
   for (size_t i = 0; i < legs.size(); ++i) {
     const LegTask& t = legs[i];
     const long long nb = (t.L * t.R + kRowTile - 1) / kRowTile;
     const size_t smem = (size_t)(kRowTile * (t.Din + 1) + t.Din * (kColTile + 1)) * sizeof(double2);
-    k_leg_apply<double><<<(unsigned)nb, kThreads, smem, stream>>>(d_legs[i], d_zero, 1, t.Din);
+    k_leg_apply<double><<<(unsigned)nb, kThreads, smem, stream>>>(&d_pack->leg[i], d_zero, 1, t.Din);
     CK(cudaGetLastError());
     note_launch(1);
   }

@@ -61,10 +61,16 @@ struct Reader {
       n *= (uint64_t)d;
       if (n > (uint64_t(1) << 36)) throw HostError(kBadFile, "checkpoint " + path + ": tensor too large");
     }
-    (void)get<std::complex<double>>();  // scale: 1 for a tensor of order >= 1
+    // the record's scale multiplies every stored element (1 in files the
+    // reference writes for tensors of order >= 1)
+    const std::complex<double> scale = get<std::complex<double>>();
+    if (!std::isfinite(scale.real()) || !std::isfinite(scale.imag()))
+      throw HostError(kBadFile, "checkpoint " + path + ": non-finite tensor scale");
     t.data.resize(n);
     f.read(reinterpret_cast<char*>(t.data.data()), (std::streamsize)(sizeof(std::complex<double>) * n));
     if (!f) throw HostError(kBadFile, "checkpoint " + path + ": unexpected end of file");
+    if (scale != std::complex<double>(1.0, 0.0))
+      for (auto& x : t.data) x *= scale;
     return t;
   }
 };
