@@ -43,7 +43,9 @@ def test_no_oracle_on_the_product_path():
 
 def test_footprint_estimate_host_only():
     """tnbp_footprint_estimate (the server's admission figure) runs without a
-    device: exact on a one-edge graph, ordered by precision, growing with D."""
+    device: exact on a one-edge graph, smallest for complex64 storage,
+    growing with D; the sweep scratch counts one wave (of at most the wave
+    budget, 96 MiB by default) rather than every site's slots."""
     tb = pytest.importorskip("tnbp_b200")
     one = tb.footprint_estimate([(0, 1)], [1], tb.C128)
     # two degree-1 sites of 2 elements x (4 x 16 B); one edge: arenas 128 B,
@@ -51,7 +53,9 @@ def test_footprint_estimate_host_only():
     assert one == int((2 * 2 * 64 + 128 + 128 + 512) * 1.1) + (8 << 20)
     e = tb.bond_square_lattice(6, 6)
     f = {p: tb.footprint_estimate(e, [16] * len(e), p) for p in (tb.C64, tb.MIXED, tb.C128)}
-    assert f[tb.C64] < f[tb.MIXED] < f[tb.C128]
+    assert f[tb.C64] < f[tb.MIXED] and f[tb.C64] < f[tb.C128]
+    # 36 sites at D = 16: all tree slots would be ~270 MB of complex128; one wave is 96 MiB
+    assert f[tb.C128] < 36 * 16**4 * 2 * 16 * 4 + (200 << 20)
     assert tb.footprint_estimate(e, [32] * len(e), tb.MIXED) > 8 * f[tb.MIXED]
     with pytest.raises(tb.TnbpError):
         tb.footprint_estimate(e, [0] * len(e), tb.MIXED)

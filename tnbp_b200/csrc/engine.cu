@@ -5,8 +5,11 @@
 // measure.cuh.  There is no CPU fallback: without a device every state call
 // fails with TNBP_ENOGPU.
 #include <cuda_runtime.h>
+#include <sys/stat.h>
 
 #include <algorithm>
+#include <cctype>
+#include <fstream>
 #include <atomic>
 #include <cmath>
 #include <complex>
@@ -30,6 +33,7 @@
 #include "tc_leg_bulk.cuh"
 #include "tc_gram.cuh"
 #include "tc_leg64.cuh"
+#include "tc_leg_gram.cuh"
 #include "trace.h"
 #include "truncate.cuh"
 
@@ -312,32 +316,14 @@ void SweepBatch::reset_graph() {
 SweepBatch& SweepBatch::operator=(SweepBatch&& o) noexcept {
   if (this != &o) {
     reset_graph();
-    levels = std::move(o.levels);
-    gram_tasks = std::move(o.gram_tasks);
-    gram_begins = std::move(o.gram_begins);
-    msg_tasks = std::move(o.msg_tasks);
-    sum_tasks = std::move(o.sum_tasks);
+    arena = std::move(o.arena);
     cond = std::move(o.cond);
-    gram_ntask = o.gram_ntask; nmsg = o.nmsg; nsum = o.nsum; gram_nblocks = o.gram_nblocks;
-    gtc_tasks = std::move(o.gtc_tasks);
-    gtc_begins = std::move(o.gtc_begins);
-    gtc_ntask = o.gtc_ntask; gtc_nblocks = o.gtc_nblocks;
-    g64_tasks = std::move(o.g64_tasks);
-    g64_begins = std::move(o.g64_begins);
-    g64_ntask = o.g64_ntask; g64_nblocks = o.g64_nblocks;
+    launches = std::move(o.launches);
     nkernels = o.nkernels;
     graph = o.graph;
     o.graph = nullptr;
   }
   return *this;
-}
-uint64_t SweepBatch::bytes() const {
-  uint64_t b = gram_tasks.bytes + gram_begins.bytes + msg_tasks.bytes + sum_tasks.bytes + cond.bytes +
-               gtc_tasks.bytes + gtc_begins.bytes + g64_tasks.bytes + g64_begins.bytes;
-  for (auto& l : levels)
-    b += l.tasks.bytes + l.begins.bytes + l.tc_tasks.bytes + l.tc_begins.bytes + l.bk_tasks.bytes +
-         l.bk_begins.bytes + l.t64_tasks.bytes + l.t64_begins.bytes;
-  return b;
 }
 
 SweepPlan::~SweepPlan() {}
@@ -352,49 +338,278 @@ uint64_t SweepPlan::bytes() const {
 // site needs 8 leg contractions instead of the 12 of the leg-by-leg
 // schedule of bp.h:137-154 (the same products in another association; the
 // per-leg normalizations of bp.h:153 only rescale, and the final
-// normalization of bp.h:166 removes the scale).
+// normalization of bp.h:166 removes the scale).  The two top-level halves
+// of a site's tree ("units") are independent: each starts from V.
 namespace {
-struct PlanOp { int site, src, dst, leg, level; };
+struct PlanOp { int site, src, dst, leg, level, unit; };
 struct SitePlanner {
   int site;
   std::vector<PlanOp>* ops;
   int next_slot = 0;
-  std::vector<int> result;  // slot holding T_t (-1 = V itself)
-  int chain(int src, int level, const std::vector<int>& legs, int* out_level) {
+  std::vector<int> result;       // slot holding T_t (-1 = V itself)
+  std::vector<int> result_unit;  // unit whose ops produce T_t
+  int chain(int src, int level, int unit, const std::vector<int>& legs, int* out_level) {
     int cur = src, lv = level;
     for (int leg : legs) {
       const int dst = next_slot++;
-      ops->push_back({site, cur, dst, leg, lv});
+      ops->push_back({site, cur, dst, leg, lv, unit});
       cur = dst;
       ++lv;
     }
     *out_level = lv;
     return cur;
   }
-  void rec(int src, int level, const std::vector<int>& targets, std::vector<char> absorbed, int g) {
+  // unit < 0: the top of the tree (its two halves become units 0 and 1)
+  void rec(int src, int level, int unit, const std::vector<int>& targets, std::vector<char> absorbed, int g) {
     if (targets.size() == 1) {
+      const int u = unit < 0 ? 0 : unit;
       std::vector<int> rest;
       for (int k = 0; k < g; ++k) if (k != targets[0] && !absorbed[k]) rest.push_back(k);
       int lv;
-      result[targets[0]] = chain(src, level, rest, &lv);
+      result[targets[0]] = chain(src, level, u, rest, &lv);
+      result_unit[targets[0]] = u;
       return;
     }
     const size_t h = targets.size() / 2;
     std::vector<int> h1(targets.begin(), targets.begin() + h), h2(targets.begin() + h, targets.end());
     for (int part = 0; part < 2; ++part) {
+      const int u = unit < 0 ? part : unit;
       const auto& keep = part == 0 ? h1 : h2;
       const auto& other = part == 0 ? h2 : h1;
       std::vector<int> legs;
       for (int k : other) if (!absorbed[k]) legs.push_back(k);
       int lv;
-      const int x = chain(src, level, legs, &lv);
+      const int x = chain(src, level, u, legs, &lv);
       auto ab = absorbed;
       for (int k : legs) ab[k] = 1;
-      rec(x, lv, keep, ab, g);
+      rec(x, lv, u, keep, ab, g);
     }
   }
 };
+
+// One unit of a site's tree with its intermediate slots mapped onto as few
+// site-sized buffers as their lifetimes allow: ops of one level run in one
+// launch, so a buffer read at level l is free for outputs of level l + 1;
+// the T_t results (or, for a fused target, the input X of its last
+// absorption) stay live until the Gram stage.  A fused target's last
+// absorption is not an op of the unit: k_leg_gram_tc does it on chip.
+struct Fused { int target, src, leg; };
+struct Unit {
+  int site = 0;
+  std::vector<PlanOp> ops;
+  std::vector<int> targets;  // targets with a plain Gram (of result[t])
+  std::vector<Fused> fused;  // targets with the fused absorption + Gram
+  std::map<int, int> buf_of_slot;
+  int nbuf = 0;
+  int nlevels = 0;
+};
+
+template <typename FuseFn>
+Unit make_unit(int site, int u, const std::vector<PlanOp>& all, const SitePlanner& sp, FuseFn fuse) {
+  Unit U;
+  U.site = site;
+  std::vector<char> skip(all.size(), 0);
+  for (size_t t = 0; t < sp.result.size(); ++t) {
+    if (sp.result_unit[t] != u) continue;
+    const int r = sp.result[t];
+    int fi = -1;
+    if (r >= 0)
+      for (size_t i = 0; i < all.size(); ++i)
+        if (all[i].site == site && all[i].dst == r) fi = (int)i;
+    if (fi >= 0 && fuse((int)t, all[fi].leg)) {
+      skip[fi] = 1;
+      U.fused.push_back({(int)t, all[fi].src, all[fi].leg});
+    } else {
+      U.targets.push_back((int)t);
+    }
+  }
+  for (size_t i = 0; i < all.size(); ++i)
+    if (all[i].site == site && all[i].unit == u && !skip[i]) U.ops.push_back(all[i]);
+  std::stable_sort(U.ops.begin(), U.ops.end(), [](const PlanOp& a, const PlanOp& b) { return a.level < b.level; });
+  constexpr int kForever = 1 << 30;
+  std::map<int, int> last_read;
+  for (const auto& op : U.ops)
+    if (op.src >= 0) last_read[op.src] = std::max(last_read[op.src], op.level);
+  for (int t : U.targets)
+    if (sp.result[t] >= 0) last_read[sp.result[t]] = kForever;
+  for (const auto& f : U.fused)
+    if (f.src >= 0) last_read[f.src] = kForever;
+  std::vector<int> busy_until;  // per buffer: last level its content is read
+  for (const auto& op : U.ops) {
+    int b = -1;
+    for (size_t i = 0; i < busy_until.size(); ++i)
+      if (busy_until[i] < op.level) { b = (int)i; break; }
+    if (b < 0) { b = (int)busy_until.size(); busy_until.push_back(0); }
+    U.buf_of_slot[op.dst] = b;
+    auto it = last_read.find(op.dst);
+    busy_until[b] = it == last_read.end() ? op.level : it->second;
+    U.nlevels = std::max(U.nlevels, op.level + 1);
+  }
+  U.nbuf = (int)busy_until.size();
+  return U;
+}
 }  // namespace
+
+// Bytes of site tensors plus intermediate slots one wave may hold; 0 puts
+// every unit of the sweep in one wave.  TNBP_WAVE_MB fixes it for every job
+// (no autotuning); otherwise a job uses the autotuned budget of its shape
+// class (below) or this default, a little under the 126 MB L2, which the
+// slots of the wave being computed share with the site tensors streaming
+// through.
+size_t wave_budget_bytes() {
+  static const size_t v = [] {
+    const char* e = std::getenv("TNBP_WAVE_MB");
+    if (e && *e) return (size_t)std::strtoull(e, nullptr, 10) << 20;
+    return size_t(96) << 20;
+  }();
+  return v;
+}
+static bool wave_budget_fixed() {
+  const char* e = std::getenv("TNBP_WAVE_MB");
+  return e && *e;
+}
+
+// ---------------------------------------------------------------- autotuner
+// The wave budget is tuned in place, per shape class and per device: the
+// first time a job of a class with a large sweep (at least 2e11 algorithmic
+// flops) starts a BP loop, each candidate budget gets a plan, one warm-up
+// sweep and two timed sweeps (CUDA events), all writing only the message
+// arena the loop overwrites next, and the fastest is kept.  The wave budget
+// only groups tasks into launches; every task's kernel and arithmetic are the
+// same under every budget, so tuning never changes a result.  Choices are
+// kept in a table per device (name and SM count) in $TNBP_TUNE_DIR (default
+// $HOME/.cache/tnbp_b200), one line per class: class, budget in MiB, best
+// and default sweep ms.  TNBP_AUTOTUNE=0 turns the tuner off.
+bool autotune_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("TNBP_AUTOTUNE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+namespace {
+constexpr size_t kWaveCandidatesMb[] = {32, 64, 96, 128, 192, 0};
+constexpr double kTuneMinFlops = 2e11;
+
+struct TuneTable {
+  std::mutex mu;
+  std::map<int, bool> loaded;                        // per device ordinal
+  std::map<int, std::map<std::string, size_t>> mb;   // device -> class -> MiB
+  std::map<int, std::string> path;
+};
+TuneTable& tune_table() {
+  static TuneTable t;
+  return t;
+}
+
+std::string tune_file(int dev) {
+  cudaDeviceProp p{};
+  CK(cudaGetDeviceProperties(&p, dev));
+  std::string name(p.name);
+  for (char& c : name)
+    if (!std::isalnum((unsigned char)c)) c = '_';
+  std::string dir;
+  if (const char* d = std::getenv("TNBP_TUNE_DIR")) dir = d;
+  else if (const char* h = std::getenv("HOME")) dir = std::string(h) + "/.cache/tnbp_b200";
+  else dir = "/tmp/tnbp_b200";
+  return dir + "/waves_" + name + "_" + std::to_string(p.multiProcessorCount) + "sm.tsv";
+}
+
+// Loads the device's table once (caller holds the mutex).
+std::map<std::string, size_t>& device_table(int dev) {
+  TuneTable& T = tune_table();
+  if (!T.loaded[dev]) {
+    T.loaded[dev] = true;
+    T.path[dev] = tune_file(dev);
+    std::ifstream f(T.path[dev]);
+    std::string key;
+    size_t mb = 0;
+    double best = 0, dflt = 0;
+    while (f >> key >> mb >> best >> dflt) T.mb[dev][key] = mb;
+  }
+  return T.mb[dev];
+}
+}  // namespace
+
+// Shape class of a job: precision, largest bond dimension, largest site
+// degree and the site count rounded up to a power of two.
+std::string Job::tune_key() const {
+  int maxd = 1, maxg = 0;
+  for (int d : dim) maxd = std::max(maxd, d);
+  for (auto& l : g.legs) maxg = std::max(maxg, (int)l.size());
+  size_t ns = 1;
+  while (ns < g.labels.size()) ns <<= 1;
+  const char* pn = prec == TNBP_C128 ? "c128" : prec == TNBP_C64 ? "c64" : "mixed";
+  return std::string(pn) + "_D" + std::to_string(maxd) + "_g" + std::to_string(maxg) + "_n" + std::to_string(ns);
+}
+
+void Job::choose_wave_budget() {
+  wave_budget = wave_budget_bytes();
+  if (wave_budget_fixed() || !autotune_enabled()) return;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  TuneTable& T = tune_table();
+  std::lock_guard<std::mutex> lk(T.mu);
+  auto& tab = device_table(dev);
+  auto it = tab.find(tune_key());
+  if (it != tab.end()) wave_budget = it->second << 20;
+}
+
+void Job::autotune_waves() {
+  if (wave_budget_fixed() || !autotune_enabled() || plan.flops < kTuneMinFlops) return;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  const std::string key = tune_key();
+  {
+    TuneTable& T = tune_table();
+    std::lock_guard<std::mutex> lk(T.mu);
+    if (device_table(dev).count(key)) return;
+  }
+  TNBP_TRACE_SCOPE("sweep.autotune");
+  struct Flag {
+    bool& f;
+    explicit Flag(bool& x) : f(x) { f = true; }
+    ~Flag() { f = false; }
+  } flag(tuning);
+  double best_ms = INFINITY, default_ms = INFINITY;
+  size_t best_mb = wave_budget_bytes() >> 20;
+  for (size_t mb : kWaveCandidatesMb) {
+    wave_budget = mb << 20;
+    destroy_graphs();
+    plan = SweepPlan();
+    build_plan();
+    run_sweep(cur);  // warm-up (and graph capture); the state is unchanged
+    double ms = 0.0;
+    for (int rep = 0; rep < 2; ++rep) {
+      run_sweep(cur);
+      CK(cudaStreamSynchronize(stream));
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, ev0, ev1));
+      ms += t;
+    }
+    if (reduced_sweeps(prec)) check_tc_error(stream);
+    ms /= 2.0;
+    if (mb == (wave_budget_bytes() >> 20)) default_ms = ms;
+    if (ms < best_ms) { best_ms = ms; best_mb = mb; }
+  }
+  wave_budget = best_mb << 20;
+  destroy_graphs();
+  plan = SweepPlan();
+  TuneTable& T = tune_table();
+  std::lock_guard<std::mutex> lk(T.mu);
+  device_table(dev)[key] = best_mb;
+  const std::string& path = T.path[dev];
+  const size_t slash = path.rfind('/');
+  if (slash != std::string::npos) {
+    // create the directory chain (best effort: an unwritable cache only
+    // means the tuning is redone by the next process)
+    for (size_t i = 1; i <= slash; ++i)
+      if (path[i] == '/') mkdir(path.substr(0, i).c_str(), 0755);
+  }
+  std::ofstream f(path, std::ios::app);
+  if (f) f << key << '\t' << best_mb << '\t' << best_ms << '\t' << default_ms << '\n';
+}
 
 void Job::build_plan() {
   TNBP_TRACE_SCOPE("sweep.build_plan");
@@ -402,59 +617,72 @@ void Job::build_plan() {
   plan = SweepPlan();
   const int ns = (int)g.labels.size();
   const int ne = (int)g.edges.size();
-  std::vector<PlanOp> ops;
+  // 1. each site's tree, split into its units
   std::vector<std::vector<int>> result(ns);
-  std::vector<int> nslots(ns, 0);
+  std::vector<Unit> units;
   for (int s = 0; s < ns; ++s) {
     const int gs = (int)g.legs[s].size();
+    std::vector<PlanOp> ops;
     SitePlanner sp;
     sp.site = s;
     sp.ops = &ops;
     sp.result.assign(gs, -1);
+    sp.result_unit.assign(gs, 0);
     std::vector<int> targets(gs);
     std::iota(targets.begin(), targets.end(), 0);
-    sp.rec(-1, 0, targets, std::vector<char>(gs, 0), gs);
+    sp.rec(-1, 0, -1, targets, std::vector<char>(gs, 0), gs);
     result[s] = sp.result;
-    nslots[s] = sp.next_slot;
+    const auto sh = site_shape(s);
+    // the last absorption of a target runs fused with its Gram on tcgen05
+    // (complex64 sweeps, both dims <= 32); decided from this job alone
+    auto fuse = [&](int t, int w) {
+      return reduced_sweeps(prec) && tcgen05_enabled() && leg_gram_enabled() && tc::leg_gram_ok(sh[t], sh[w]);
+    };
+    const int nunits = gs >= 2 ? 2 : 1;
+    for (int u = 0; u < nunits; ++u) units.push_back(make_unit(s, u, ops, sp, fuse));
   }
-  // scratch: every slot of a site holds one site-sized tensor
-  std::vector<size_t> slot_base(ns, 0);
-  size_t o = 0;
-  for (int s = 0; s < ns; ++s) { slot_base[s] = o; o += (size_t)nslots[s] * align_elems(site_elems(s)); }
-  ws_scratch.ensure(std::max<size_t>(o, 32) * wsz, stream);
-  auto slot_ptr = [&](int s, int slot) -> void* {
-    if (slot < 0) return sweep_vptr(s);
-    return static_cast<char*>(ws_scratch.p) + (slot_base[s] + (size_t)slot * align_elems(site_elems(s))) * wsz;
+  // 2. waves of consecutive units within the byte budget (at least one unit)
+  if (!tuning) choose_wave_budget();
+  const size_t budget = wave_budget;
+  std::vector<std::vector<int>> waves;
+  {
+    size_t bytes = 0;
+    int last_site = -1;
+    for (size_t i = 0; i < units.size(); ++i) {
+      const Unit& U = units[i];
+      const size_t site_b = align_elems(site_elems(U.site)) * wsz;
+      const size_t add = (size_t)U.nbuf * site_b + (U.site == last_site ? 0 : site_b);
+      if (waves.empty() || (budget && bytes + add > budget && !waves.back().empty())) {
+        waves.emplace_back();
+        bytes = site_b + (size_t)U.nbuf * site_b;
+      } else {
+        bytes += add;
+      }
+      waves.back().push_back((int)i);
+      last_site = U.site;
+    }
+  }
+  // 3. slot buffers: a wave's units side by side, every wave at offset 0
+  std::vector<size_t> unit_base(units.size(), 0);
+  size_t scratch = 0;
+  for (auto& w : waves) {
+    size_t o = 0;
+    for (int ui : w) {
+      unit_base[ui] = o;
+      o += (size_t)units[ui].nbuf * align_elems(site_elems(units[ui].site));
+    }
+    scratch = std::max(scratch, o);
+  }
+  ws_scratch.ensure(std::max<size_t>(scratch, 32) * wsz, stream);
+  auto slot_ptr = [&](int ui, int slot) -> void* {
+    const Unit& U = units[ui];
+    if (slot < 0) return sweep_vptr(U.site);
+    return static_cast<char*>(ws_scratch.p) +
+           (unit_base[ui] + (size_t)U.buf_of_slot.at(slot) * align_elems(site_elems(U.site))) * wsz;
   };
-  int maxlevel = 0;
-  for (auto& op : ops) maxlevel = std::max(maxlevel, op.level + 1);
-  plan.levels.assign(maxlevel, LevelHost());
+  // 4. tasks
   plan.flops = 0.0;
   plan.bytes_alg = 0.0;
-  for (auto& op : ops) {
-    const auto sh = site_shape(op.site);
-    long long L = 1, R = 1;
-    for (int k = 0; k < op.leg; ++k) L *= sh[k];
-    for (size_t k = op.leg + 1; k < sh.size(); ++k) R *= sh[k];
-    const int D = sh[op.leg];
-    auto& lvh = plan.levels[op.level];
-    for (int par = 0; par < 2; ++par) {
-      LegTask lt;
-      lt.in = slot_ptr(op.site, op.src);
-      lt.out = slot_ptr(op.site, op.dst);
-      lt.mat = mptr(par, g.in_msg(op.site, op.leg));
-      lt.L = L; lt.R = R; lt.Din = D; lt.Dout = D;
-      lt.block_begin = 0;  // assigned when a batch is built
-      lvh.tasks[par].push_back(lt);
-    }
-    lvh.max_din = std::max(lvh.max_din, D);
-  }
-  // Gram + finalize tasks, one per directed message
-  size_t part_elems = 0;
-  struct Pending { int s, t; size_t part_off; };
-  std::vector<Pending> pend;
-  plan.gram.clear();
-  plan.gram_blocks.clear();
   for (int s = 0; s < ns; ++s) {
     const auto sh = site_shape(s);
     const int gs = (int)g.legs[s].size();
@@ -464,42 +692,119 @@ void Job::build_plan() {
     // algorithmic work of bp.h's schedule: 8 d prod(D) sum(D) flops per message
     plan.flops += gs * 8.0 * n * sumD;
     plan.bytes_alg += n * wsz;  // each site tensor read once (as the sweep reads it)
-    for (int t = 0; t < gs; ++t) {
-      GramTask g1;
-      g1.A = slot_ptr(s, result[s][t]);
-      g1.B = sweep_vptr(s);
-      long long L = 1, M = 1;
-      for (int k = 0; k < t; ++k) L *= sh[k];
-      for (size_t k = t + 1; k < sh.size(); ++k) M *= sh[k];
-      g1.L = L; g1.M = M; g1.D = sh[t]; g1.P = 1; g1.C = sh[t];
-      g1.ctiles = (g1.C + kColTile - 1) / kColTile;
-      g1.Q = L * M;
-      long long cr = ((g1.Q / 16) + kRowTile - 1) / kRowTile * kRowTile;
-      cr = std::max<long long>(256, std::min<long long>(4096, cr));
-      g1.chunk_rows = cr;
-      g1.nchunk = (int)((g1.Q + cr - 1) / cr);
-      g1.partial = nullptr;
-      g1.block_begin = 0;
-      pend.push_back({s, t, part_elems});
-      part_elems += (size_t)g1.nchunk * g1.C * g1.C;
-      plan.gram.push_back(g1);
-      plan.gram_blocks.push_back((long long)g1.nchunk * g1.ctiles * g1.ctiles);
-      plan.bytes_alg += 2.0 * sh[t] * sh[t] * esz;  // message in + out
-    }
+    for (int t = 0; t < gs; ++t) plan.bytes_alg += 2.0 * sh[t] * sh[t] * esz;  // message in + out
   }
-  plan.partial.alloc(std::max<size_t>(part_elems, 1) * sizeof(double2), stream);
+  plan.waves.assign(waves.size(), WaveHost());
+  size_t max_part = 1;
+  struct Pending { int s, t; size_t part_off; int nchunk, C; };
+  std::vector<Pending> pend;      // one per target, in message order
+  std::vector<size_t> gram_part;  // pend index of each plain Gram task
+  std::vector<size_t> lg_part;    // pend index of each fused task
+  for (size_t w = 0; w < waves.size(); ++w) {
+    WaveHost& W = plan.waves[w];
+    int nlev = 0;
+    for (int ui : waves[w]) nlev = std::max(nlev, units[ui].nlevels);
+    W.levels.assign(nlev, LevelHost());
+    size_t part = 0;
+    for (int ui : waves[w]) {
+      const Unit& U = units[ui];
+      const auto sh = site_shape(U.site);
+      for (const auto& op : U.ops) {
+        long long L = 1, R = 1;
+        for (int k = 0; k < op.leg; ++k) L *= sh[k];
+        for (size_t k = op.leg + 1; k < sh.size(); ++k) R *= sh[k];
+        for (int par = 0; par < 2; ++par) {
+          LegTask lt;
+          lt.in = slot_ptr(ui, op.src);
+          lt.out = slot_ptr(ui, op.dst);
+          lt.mat = mptr(par, g.in_msg(op.site, op.leg));
+          lt.L = L; lt.R = R; lt.Din = sh[op.leg]; lt.Dout = sh[op.leg];
+          lt.block_begin = 0;  // assigned when a batch is built
+          W.levels[op.level].tasks[par].push_back(lt);
+        }
+      }
+      for (int t : U.targets) {
+        GramTask g1;
+        g1.A = slot_ptr(ui, result[U.site][t]);
+        g1.B = sweep_vptr(U.site);
+        long long L = 1, M = 1;
+        for (int k = 0; k < t; ++k) L *= sh[k];
+        for (size_t k = t + 1; k < sh.size(); ++k) M *= sh[k];
+        g1.L = L; g1.M = M; g1.D = sh[t]; g1.P = 1; g1.C = sh[t];
+        g1.ctiles = (g1.C + kColTile - 1) / kColTile;
+        g1.Q = L * M;
+        // chunks of at most Q/128 rows (multiples of 64), so that even a
+        // wave of one unit gives every SM Gram work
+        long long cr = ((g1.Q / 128) + 63) / 64 * 64;
+        cr = std::max<long long>(256, std::min<long long>(4096, cr));
+        g1.chunk_rows = cr;
+        g1.nchunk = (int)((g1.Q + cr - 1) / cr);
+        g1.partial = nullptr;
+        g1.block_begin = 0;
+        W.grams.push_back((int)plan.gram.size());
+        W.msgs.push_back((int)pend.size());
+        gram_part.push_back(pend.size());
+        pend.push_back({U.site, t, part, g1.nchunk, g1.C});
+        part += (size_t)g1.nchunk * g1.C * g1.C;
+        plan.gram.push_back(g1);
+        plan.gram_blocks.push_back((long long)g1.nchunk * g1.ctiles * g1.ctiles);
+      }
+      for (const auto& f : U.fused) {
+        const int t = f.target, w2 = f.leg, p1 = std::min(t, w2), p2 = std::max(t, w2);
+        long long L1 = 1, Mid = 1, R = 1;
+        for (int k = 0; k < p1; ++k) L1 *= sh[k];
+        for (int k = p1 + 1; k < p2; ++k) Mid *= sh[k];
+        for (size_t k = p2 + 1; k < sh.size(); ++k) R *= sh[k];
+        LegGramTask lg;
+        lg.X = slot_ptr(ui, f.src);
+        lg.V = sweep_vptr(U.site);
+        lg.E = nullptr;  // per parity below
+        lg.st = 1; lg.sw = 1;
+        for (int k = 0; k < t; ++k) lg.st *= sh[k];
+        for (int k = 0; k < w2; ++k) lg.sw *= sh[k];
+        lg.L1 = L1; lg.Mid = Mid;
+        lg.s_mid = L1 * sh[p1];
+        lg.s_r = L1 * sh[p1] * Mid * sh[p2];
+        lg.n_outer = L1 * Mid * R;
+        lg.Dt = sh[t]; lg.Dw = sh[w2];
+        // thread order along the unit-stride index: c (t = leg 0), j
+        // (w = leg 0) or the outer index
+        lg.mode = t == 0 ? 0 : (w2 == 0 ? 1 : 2);
+        const long long tiles = (lg.n_outer + tc::kLgOuter - 1) / tc::kLgOuter;
+        lg.chunk_tiles = (int)std::max<long long>(1, std::min<long long>(16, tiles / 128));
+        lg.nchunk = (int)((tiles + lg.chunk_tiles - 1) / lg.chunk_tiles);
+        lg.partial = nullptr;
+        lg.block_begin = 0;
+        W.lgs.push_back((int)plan.lg[0].size());
+        W.msgs.push_back((int)pend.size());
+        lg_part.push_back(pend.size());
+        pend.push_back({U.site, t, part, lg.nchunk, lg.Dt});
+        part += (size_t)lg.nchunk * lg.Dt * lg.Dt;
+        for (int par = 0; par < 2; ++par) {
+          LegGramTask l2 = lg;
+          l2.E = mptr(par, g.in_msg(U.site, w2));
+          plan.lg[par].push_back(l2);
+        }
+      }
+    }
+    max_part = std::max(max_part, part);
+  }
+  // Gram partials are finalized at the end of their wave, so one wave's
+  // worth of partials is enough
+  plan.partial.alloc(max_part * sizeof(double2), stream);
   plan.dist.alloc(std::max<size_t>(2 * ne, 1) * sizeof(double), stream);
-  double2* part = static_cast<double2*>(plan.partial.p);
-  plan.msg[0].clear();
-  plan.msg[1].clear();
-  for (size_t i = 0; i < plan.gram.size(); ++i) {
-    plan.gram[i].partial = part + pend[i].part_off;
+  double2* partial = static_cast<double2*>(plan.partial.p);
+  for (size_t i = 0; i < plan.gram.size(); ++i) plan.gram[i].partial = partial + pend[gram_part[i]].part_off;
+  for (size_t i = 0; i < lg_part.size(); ++i)
+    for (int par = 0; par < 2; ++par) plan.lg[par][i].partial = partial + pend[lg_part[i]].part_off;
+  for (int par = 0; par < 2; ++par) plan.msg[par].clear();
+  for (size_t i = 0; i < pend.size(); ++i) {
     const int mo = g.out_msg(pend[i].s, pend[i].t);
     for (int par = 0; par < 2; ++par) {
       MsgTask m;
-      m.partial = plan.gram[i].partial;
-      m.nchunk = plan.gram[i].nchunk;
-      m.C = plan.gram[i].C;
+      m.partial = partial + pend[i].part_off;
+      m.nchunk = pend[i].nchunk;
+      m.C = pend[i].C;
       m.out = mptr(1 - par, mo);
       m.old = mptr(par, mo);
       m.dist = static_cast<double*>(plan.dist.p) + mo;
@@ -508,23 +813,45 @@ void Job::build_plan() {
     }
   }
   plan.valid = true;
-  for (int par = 0; par < 2; ++par) build_batch({{this, par}}, plan.single[par], stream);
+  static std::atomic<uint64_t> serials{0};
+  plan_serial = ++serials;
+  // the per-job launch sequences (plan.single) are built on first use: a
+  // served job only ever runs inside batches
   CK(cudaStreamSynchronize(stream));
   check_budget();
 }
 
 // Concatenate the sweep tasks of several jobs (each at its own message
-// parity) into one set of launches; block offsets are re-based so uneven
-// jobs share every launch.
+// parity) into one launch sequence: wave k of the batch holds wave k of
+// every job, block offsets are re-based so uneven jobs share every launch,
+// and all task arrays go to the device in one copy.
 void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStream_t stream) {
   TNBP_TRACE_SCOPE("sweep.build_batch");
   b.reset_graph();
-  size_t nlev = 0;
+  b.launches.clear();
+  size_t nw = 0;
   for (auto& e : entries) {
     if (!e.job->plan.valid) e.job->build_plan();
-    nlev = std::max(nlev, e.job->plan.levels.size());
+    nw = std::max(nw, e.job->plan.waves.size());
   }
-  b.levels.resize(nlev);
+  std::vector<unsigned char> host;
+  auto put = [&](const void* p, size_t bytes) -> size_t {
+    const size_t off = (host.size() + 255) & ~size_t(255);
+    host.resize(off + std::max<size_t>(bytes, 16));
+    if (bytes) std::memcpy(host.data() + off, p, bytes);
+    return off;
+  };
+  auto add = [&](int kind, const auto& tasks, const std::vector<long long>& begins, long long nblocks, int max_din) {
+    if (tasks.empty()) return;
+    SweepLaunch L;
+    L.kind = kind;
+    L.tasks_off = put(tasks.data(), tasks.size() * sizeof(tasks[0]));
+    L.begins_off = begins.empty() ? 0 : put(begins.data(), begins.size() * sizeof(long long));
+    L.ntask = (int)tasks.size();
+    L.nblocks = nblocks;
+    L.max_din = max_din;
+    b.launches.push_back(L);
+  };
   // The kernel is chosen per task, never per launch: complex64 tasks whose
   // tile is a contiguous byte range (tc::bulk_mode) run on the bulk-staged
   // tcgen05 kernel, other tasks with Din, Dout <= 32 on the register-staged
@@ -532,115 +859,109 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
   // shares the batch.  A request's rounding therefore does not depend on
   // what it is batched with.
   const bool tc_ok = !entries.empty() && reduced_sweeps(entries[0].job->prec) && tcgen05_enabled();
-  for (size_t lv = 0; lv < nlev; ++lv) {
-    std::vector<LegTask> t, t2, t3, t4;
-    std::vector<long long> beg, b2, b3, b4;
-    long long nb = 0, nb2 = 0, nb3 = 0, nb4 = 0;
-    int maxdin = 1;
+  for (size_t w = 0; w < nw; ++w) {
+    size_t nlev = 0;
+    for (auto& e : entries)
+      if (w < e.job->plan.waves.size()) nlev = std::max(nlev, e.job->plan.waves[w].levels.size());
+    for (size_t lv = 0; lv < nlev; ++lv) {
+      std::vector<LegTask> t, t2, t3, t4;
+      std::vector<long long> beg, b2, b3, b4;
+      long long nb = 0, nb2 = 0, nb3 = 0, nb4 = 0;
+      int maxdin = 1;
+      for (auto& e : entries) {
+        const auto& P = e.job->plan;
+        if (w >= P.waves.size() || lv >= P.waves[w].levels.size()) continue;
+        for (LegTask lt : P.waves[w].levels[lv].tasks[e.parity]) {
+          if (tc_ok && bulk_leg_enabled() && tc::bulk_mode(lt.L, lt.Din, lt.Dout) != 0) {
+            lt.block_begin = nb3;
+            b3.push_back(nb3);
+            nb3 += (lt.L * lt.R + tc::kTcRows - 1) / tc::kTcRows;
+            t3.push_back(lt);
+          } else if (tc_ok && tc::leg64_ok(lt.Din, lt.Dout)) {
+            lt.block_begin = nb4;
+            b4.push_back(nb4);
+            nb4 += (lt.L * lt.R + tc::kTcRows - 1) / tc::kTcRows;
+            t4.push_back(lt);
+          } else if (tc_ok && lt.Din <= tc::kTcMaxD && lt.Dout <= tc::kTcMaxD) {
+            lt.block_begin = nb2;
+            b2.push_back(nb2);
+            nb2 += (lt.L * lt.R + tc::kTcRows - 1) / tc::kTcRows;
+            t2.push_back(lt);
+          } else {
+            lt.block_begin = nb;
+            beg.push_back(nb);
+            nb += (lt.L * lt.R + kRowTile - 1) / kRowTile;
+            maxdin = std::max(maxdin, lt.Din);
+            t.push_back(lt);
+          }
+        }
+      }
+      add(SweepLaunch::LEG_BULK, t3, b3, nb3, 0);
+      add(SweepLaunch::LEG_T64, t4, b4, nb4, 0);
+      add(SweepLaunch::LEG_TC, t2, b2, nb2, 0);
+      add(SweepLaunch::LEG_CORE, t, beg, nb, maxdin);
+    }
+    // Gram tasks: the fused absorption + Gram kernel, then per task the
+    // tcgen05 kernels (one CTA per chunk) for the complex64 sweeps with C <=
+    // 64, else the CUDA-core kernel; then the wave's messages are finalized
+    std::vector<GramTask> gt, gt2, gt3;
+    std::vector<long long> gb, gb2, gb3, lb;
+    std::vector<LegGramTask> lt;
+    std::vector<MsgTask> mt;
+    long long nb = 0, nb2 = 0, nb3 = 0, nlb = 0;
     for (auto& e : entries) {
       const auto& P = e.job->plan;
-      if (lv >= P.levels.size()) continue;
-      for (LegTask lt : P.levels[lv].tasks[e.parity]) {
-        if (tc_ok && bulk_leg_enabled() && tc::bulk_mode(lt.L, lt.Din, lt.Dout) != 0) {
-          lt.block_begin = nb3;
-          b3.push_back(nb3);
-          nb3 += (lt.L * lt.R + tc::kTcRows - 1) / tc::kTcRows;
-          t3.push_back(lt);
-        } else if (tc_ok && tc::leg64_ok(lt.Din, lt.Dout)) {
-          lt.block_begin = nb4;
-          b4.push_back(nb4);
-          nb4 += (lt.L * lt.R + tc::kTcRows - 1) / tc::kTcRows;
-          t4.push_back(lt);
-        } else if (tc_ok && lt.Din <= tc::kTcMaxD && lt.Dout <= tc::kTcMaxD) {
-          lt.block_begin = nb2;
-          b2.push_back(nb2);
-          nb2 += (lt.L * lt.R + tc::kTcRows - 1) / tc::kTcRows;
-          t2.push_back(lt);
+      if (w >= P.waves.size()) continue;
+      for (int li : P.waves[w].lgs) {
+        LegGramTask l1 = P.lg[e.parity][li];
+        l1.block_begin = nlb;
+        lb.push_back(nlb);
+        nlb += l1.nchunk;
+        lt.push_back(l1);
+      }
+      for (int mi : P.waves[w].msgs) mt.push_back(P.msg[e.parity][mi]);
+      for (int gi : P.waves[w].grams) {
+        GramTask g1 = P.gram[gi];
+        if (tc_ok && tc::gram_tc_ok(g1.C, g1.P)) {
+          g1.block_begin = nb2;
+          gb2.push_back(nb2);
+          nb2 += g1.nchunk;
+          gt2.push_back(g1);
+        } else if (tc_ok && tc::gram64_ok(g1.C, g1.P)) {
+          g1.block_begin = nb3;
+          gb3.push_back(nb3);
+          nb3 += g1.nchunk;
+          gt3.push_back(g1);
         } else {
-          lt.block_begin = nb;
-          beg.push_back(nb);
-          nb += (lt.L * lt.R + kRowTile - 1) / kRowTile;
-          maxdin = std::max(maxdin, lt.Din);
-          t.push_back(lt);
+          g1.block_begin = nb;
+          gb.push_back(nb);
+          nb += P.gram_blocks[gi];
+          gt.push_back(g1);
         }
       }
     }
-    SweepBatch::Level& L = b.levels[lv];
-    upload_vec(L.tasks, t, stream);
-    upload_vec(L.begins, beg, stream);
-    L.ntask = (int)t.size();
-    L.nblocks = nb;
-    L.max_din = maxdin;
-    upload_vec(L.tc_tasks, t2, stream);
-    upload_vec(L.tc_begins, b2, stream);
-    L.tc_ntask = (int)t2.size();
-    L.tc_nblocks = nb2;
-    L.tc_smem = tc::leg_smem_bytes();
-    upload_vec(L.bk_tasks, t3, stream);
-    upload_vec(L.bk_begins, b3, stream);
-    L.bk_ntask = (int)t3.size();
-    L.bk_nblocks = nb3;
-    upload_vec(L.t64_tasks, t4, stream);
-    upload_vec(L.t64_begins, b4, stream);
-    L.t64_ntask = (int)t4.size();
-    L.t64_nblocks = nb4;
+    add(SweepLaunch::LEG_GRAM, lt, lb, nlb, 0);
+    add(SweepLaunch::GRAM_TC, gt2, gb2, nb2, 0);
+    add(SweepLaunch::GRAM_T64, gt3, gb3, nb3, 0);
+    add(SweepLaunch::GRAM_CORE, gt, gb, nb, 0);
+    add(SweepLaunch::MSG, mt, {}, (long long)mt.size(), 0);
   }
-  // Gram tasks: per task, the tcgen05 kernel (one CTA per chunk) for the
-  // complex64 sweeps with C <= 32, else the CUDA-core kernel
-  std::vector<GramTask> gt, gt2, gt3;
-  std::vector<long long> gb, gb2, gb3;
-  std::vector<MsgTask> mt;
+  // one condition per job
+  b.cond.ensure(std::max<size_t>(entries.size(), 1) * sizeof(double), stream);
   std::vector<SumTask> st;
-  long long nb = 0, nb2 = 0, nb3 = 0;
   for (size_t ei = 0; ei < entries.size(); ++ei) {
     const auto& P = entries[ei].job->plan;
-    for (size_t i = 0; i < P.gram.size(); ++i) {
-      GramTask g1 = P.gram[i];
-      if (tc_ok && tc::gram_tc_ok(g1.C, g1.P)) {
-        g1.block_begin = nb2;
-        gb2.push_back(nb2);
-        nb2 += g1.nchunk;
-        gt2.push_back(g1);
-        continue;
-      }
-      if (tc_ok && tc::gram64_ok(g1.C, g1.P)) {
-        g1.block_begin = nb3;
-        gb3.push_back(nb3);
-        nb3 += g1.nchunk;
-        gt3.push_back(g1);
-        continue;
-      }
-      g1.block_begin = nb;
-      gb.push_back(nb);
-      nb += P.gram_blocks[i];
-      gt.push_back(g1);
-    }
-    for (auto& m : P.msg[entries[ei].parity]) mt.push_back(m);
     SumTask s1;
     s1.x = static_cast<const double*>(P.dist.p);
     s1.n = (int)P.msg[0].size();
     s1.scale = 1.0 / (2.0 * (double)entries[ei].job->g.edges.size());
-    s1.out = nullptr;  // patched after cond is allocated
+    s1.out = static_cast<double*>(b.cond.p) + ei;
     st.push_back(s1);
   }
-  b.cond.alloc(std::max<size_t>(entries.size(), 1) * sizeof(double), stream);
-  for (size_t i = 0; i < st.size(); ++i) st[i].out = static_cast<double*>(b.cond.p) + i;
-  upload_vec(b.gram_tasks, gt, stream);
-  upload_vec(b.gram_begins, gb, stream);
-  upload_vec(b.msg_tasks, mt, stream);
-  upload_vec(b.sum_tasks, st, stream);
-  b.gram_ntask = (int)gt.size();
-  b.gram_nblocks = nb;
-  upload_vec(b.gtc_tasks, gt2, stream);
-  upload_vec(b.gtc_begins, gb2, stream);
-  b.gtc_ntask = (int)gt2.size();
-  b.gtc_nblocks = nb2;
-  upload_vec(b.g64_tasks, gt3, stream);
-  upload_vec(b.g64_begins, gb3, stream);
-  b.g64_ntask = (int)gt3.size();
-  b.g64_nblocks = nb3;
-  b.nmsg = (int)mt.size();
-  b.nsum = (int)st.size();
+  add(SweepLaunch::SUM, st, {}, (long long)st.size(), 0);
+  b.arena.ensure(std::max<size_t>(host.size(), 256), stream);
+  CK(cudaMemcpyAsync(b.arena.p, host.data(), host.size(), cudaMemcpyHostToDevice, stream));
+  b.nkernels = (int)b.launches.size();
 }
 
 template <typename R>
@@ -660,72 +981,63 @@ static void leg_apply_attr() {
 
 template <typename R, typename MR>
 static int launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
-  int n = 0;
-  for (auto& lv : b.levels) {
-    if (lv.bk_ntask > 0) {
-      // persistent: one CTA per SM (about 193 KB of shared memory each)
-      const long long grid = std::min<long long>(lv.bk_nblocks, num_sms());
-      k_leg_apply_tc_bulk<MR><<<(unsigned)grid, 256, tc::bulk_smem_bytes(), stream>>>(
-          static_cast<const LegTask*>(lv.bk_tasks.p), static_cast<const long long*>(lv.bk_begins.p), lv.bk_ntask,
-          lv.bk_nblocks);
-      CK(cudaGetLastError());
-      ++n;
+  const char* base = static_cast<const char*>(b.arena.p);
+  for (const SweepLaunch& L : b.launches) {
+    const void* tasks = base + L.tasks_off;
+    const long long* begins = reinterpret_cast<const long long*>(base + L.begins_off);
+    switch (L.kind) {
+      case SweepLaunch::LEG_BULK: {
+        // persistent: one CTA per SM (about 193 KB of shared memory each)
+        const long long grid = std::min<long long>(L.nblocks, num_sms());
+        k_leg_apply_tc_bulk<MR><<<(unsigned)grid, 256, tc::bulk_smem_bytes(), stream>>>(
+            static_cast<const LegTask*>(tasks), begins, L.ntask, L.nblocks);
+        break;
+      }
+      case SweepLaunch::LEG_T64: {
+        // persistent: one 256-thread CTA per SM (about 193 KB of shared memory)
+        const long long grid = std::min<long long>(L.nblocks, num_sms());
+        k_leg_apply_tc64<MR><<<(unsigned)grid, 256, tc::leg64_smem_bytes(), stream>>>(
+            static_cast<const LegTask*>(tasks), begins, L.ntask, L.nblocks);
+        break;
+      }
+      case SweepLaunch::LEG_TC: {
+        // persistent: up to 2 CTAs per SM, each over a contiguous range of tiles
+        const long long grid = std::min<long long>(L.nblocks, 2LL * num_sms());
+        k_leg_apply_tc<MR><<<(unsigned)grid, 128, tc::leg_smem_bytes(), stream>>>(
+            static_cast<const LegTask*>(tasks), begins, L.ntask, L.nblocks);
+        break;
+      }
+      case SweepLaunch::LEG_CORE: {
+        if (L.max_din > 128) throw Error(TNBP_EUNSUPPORTED, "bond dimension above 128 during BP");
+        k_leg_apply<R, MR><<<(unsigned)L.nblocks, kThreads, leg_smem<R>(L.max_din), stream>>>(
+            static_cast<const LegTask*>(tasks), begins, L.ntask, L.max_din);
+        break;
+      }
+      case SweepLaunch::GRAM_TC:
+        k_gram_tc<<<(unsigned)L.nblocks, 256, tc::gram_smem_bytes(), stream>>>(
+            static_cast<const GramTask*>(tasks), begins, L.ntask);
+        break;
+      case SweepLaunch::GRAM_T64:
+        k_gram_tc64<<<(unsigned)L.nblocks, 256, tc::gram64_smem_bytes(), stream>>>(
+            static_cast<const GramTask*>(tasks), begins, L.ntask);
+        break;
+      case SweepLaunch::LEG_GRAM:
+        k_leg_gram_tc<MR><<<(unsigned)L.nblocks, 256, tc::leg_gram_smem_bytes(), stream>>>(
+            static_cast<const LegGramTask*>(tasks), begins, L.ntask);
+        break;
+      case SweepLaunch::GRAM_CORE:
+        k_gram<R><<<(unsigned)L.nblocks, kThreads, 0, stream>>>(static_cast<const GramTask*>(tasks), begins, L.ntask);
+        break;
+      case SweepLaunch::MSG:
+        k_msg_finalize<R, MR><<<L.ntask, kThreads, 0, stream>>>(static_cast<const MsgTask*>(tasks));
+        break;
+      case SweepLaunch::SUM:
+        k_segmented_sum<<<L.ntask, kThreads, 0, stream>>>(static_cast<const SumTask*>(tasks));
+        break;
     }
-    if (lv.t64_ntask > 0) {
-      // persistent: one 256-thread CTA per SM (about 193 KB of shared memory)
-      const long long grid = std::min<long long>(lv.t64_nblocks, num_sms());
-      k_leg_apply_tc64<MR><<<(unsigned)grid, 256, tc::leg64_smem_bytes(), stream>>>(
-          static_cast<const LegTask*>(lv.t64_tasks.p), static_cast<const long long*>(lv.t64_begins.p),
-          lv.t64_ntask, lv.t64_nblocks);
-      CK(cudaGetLastError());
-      ++n;
-    }
-    if (lv.tc_ntask > 0) {
-      // persistent: up to 2 CTAs per SM, each over a contiguous range of tiles
-      const long long grid = std::min<long long>(lv.tc_nblocks, 2LL * num_sms());
-      k_leg_apply_tc<MR><<<(unsigned)grid, 128, lv.tc_smem, stream>>>(
-          static_cast<const LegTask*>(lv.tc_tasks.p), static_cast<const long long*>(lv.tc_begins.p), lv.tc_ntask,
-          lv.tc_nblocks);
-      CK(cudaGetLastError());
-      ++n;
-    }
-    if (lv.ntask == 0) continue;
-    if (lv.max_din > 128) throw Error(TNBP_EUNSUPPORTED, "bond dimension above 128 during BP");
-    const size_t smem = leg_smem<R>(lv.max_din);
-    k_leg_apply<R, MR><<<(unsigned)lv.nblocks, kThreads, smem, stream>>>(
-        static_cast<const LegTask*>(lv.tasks.p), static_cast<const long long*>(lv.begins.p), lv.ntask, lv.max_din);
     CK(cudaGetLastError());
-    ++n;
   }
-  if (b.gtc_ntask) {
-    k_gram_tc<<<(unsigned)b.gtc_nblocks, 256, tc::gram_smem_bytes(), stream>>>(
-        static_cast<const GramTask*>(b.gtc_tasks.p), static_cast<const long long*>(b.gtc_begins.p), b.gtc_ntask);
-    CK(cudaGetLastError());
-    ++n;
-  }
-  if (b.g64_ntask) {
-    k_gram_tc64<<<(unsigned)b.g64_nblocks, 256, tc::gram64_smem_bytes(), stream>>>(
-        static_cast<const GramTask*>(b.g64_tasks.p), static_cast<const long long*>(b.g64_begins.p), b.g64_ntask);
-    CK(cudaGetLastError());
-    ++n;
-  }
-  if (b.gram_ntask) {
-    k_gram<R><<<(unsigned)b.gram_nblocks, kThreads, 0, stream>>>(
-        static_cast<const GramTask*>(b.gram_tasks.p), static_cast<const long long*>(b.gram_begins.p), b.gram_ntask);
-    CK(cudaGetLastError());
-    ++n;
-  }
-  if (b.nmsg) {
-    k_msg_finalize<R, MR><<<b.nmsg, kThreads, 0, stream>>>(static_cast<const MsgTask*>(b.msg_tasks.p));
-    CK(cudaGetLastError());
-    ++n;
-  }
-  if (b.nsum) {
-    k_segmented_sum<<<b.nsum, kThreads, 0, stream>>>(static_cast<const SumTask*>(b.sum_tasks.p));
-    CK(cudaGetLastError());
-    ++n;
-  }
-  return n;
+  return (int)b.launches.size();
 }
 
 // Sweep kernels: TNBP_C128 all complex128; TNBP_C64 all complex64;
@@ -747,6 +1059,8 @@ static void tc_attr() {
                           (int)tc::bulk_smem_bytes()));
   CK(cudaFuncSetAttribute(k_leg_apply_tc64<MR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)tc::leg64_smem_bytes()));
+  CK(cudaFuncSetAttribute(k_leg_gram_tc<MR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)tc::leg_gram_smem_bytes()));
   if (!attr_done(gram_flags)) {
     CK(cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::gram_smem_bytes()));
     CK(cudaFuncSetAttribute(k_gram_tc64, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -802,6 +1116,18 @@ bool bulk_leg_enabled() {
   return on;
 }
 
+// The last absorption of every target with dims <= 32 runs fused with its
+// Gram (k_leg_gram_tc) on the reduced-precision paths; TNBP_LEG_GRAM=0
+// returns those targets to the separate leg and Gram kernels (both compute
+// the same contraction; used to compare the two).
+bool leg_gram_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("TNBP_LEG_GRAM");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 // A tcgen05 CTA that gave up waiting for its MMAs records it in g_tc_error.
 void check_tc_error(cudaStream_t stream) {
   int err = 0;
@@ -819,6 +1145,7 @@ void Job::run_sweep(int par) {
   sync_shadow();
   if (!plan.valid) build_plan();
   SweepBatch& b = plan.single[par];
+  if (b.launches.empty()) build_batch({{this, par}}, b, stream);
   if (!b.graph) {
     TNBP_TRACE_SCOPE("sweep.graph_capture");
     prepare_kernels(prec);
@@ -896,6 +1223,9 @@ void Job::bp_run(double tol_in, int max_iter, int* iters, double* cond) {
   *iters = 0;
   *cond = std::nan("");
   if (max_iter <= 0) return;
+  sync_shadow();
+  if (!plan.valid) build_plan();
+  autotune_waves();
   run_sweep(cur);
   cur = 1 - cur;
   *iters = 1;

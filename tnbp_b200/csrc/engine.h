@@ -69,41 +69,37 @@ struct Graph {
 
 struct LevelHost {
   std::vector<LegTask> tasks[2];  // per message-arena parity
-  int max_din = 1;
+};
+
+// One wave of a sweep: whole half-trees ("units") of consecutive sites whose
+// site tensors and intermediate slots fit a byte budget, so that a unit's
+// slots are written and read back while they are still in L2.  A wave runs
+// its levels in order, then its Gram tasks, then the finalization of its
+// messages; the next wave reuses the same slot and partial buffers.
+struct WaveHost {
+  std::vector<LevelHost> levels;
+  std::vector<int> grams;  // indices into SweepPlan::gram
+  std::vector<int> lgs;    // indices into SweepPlan::lg
+  std::vector<int> msgs;   // indices into SweepPlan::msg (one per target)
+};
+
+// One kernel launch of a sweep batch; its task arrays live in the batch's
+// arena at the given byte offsets.
+struct SweepLaunch {
+  enum Kind { LEG_BULK, LEG_T64, LEG_TC, LEG_CORE, GRAM_TC, GRAM_T64, GRAM_CORE, LEG_GRAM, MSG, SUM };
+  int kind;
+  size_t tasks_off, begins_off;
+  int ntask;
+  long long nblocks;
+  int max_din;
 };
 
 // Device task arrays of one sweep launch sequence; built from one job (the
 // per-job path, captured once per parity as a CUDA graph) or from many jobs
 // at once (the served path: every active job's sweep in the same launches).
 struct SweepBatch {
-  struct Level {
-    DevBuf tasks, begins;
-    int ntask = 0;
-    long long nblocks = 0;
-    int max_din = 1;
-    // tasks of the tcgen05 kernel (complex64, Din and Dout <= 32): 128-row
-    // tiles; the fields above hold the level's other tasks
-    DevBuf tc_tasks, tc_begins;
-    int tc_ntask = 0;
-    long long tc_nblocks = 0;
-    // tasks of the bulk-staged tcgen05 kernel (tc::bulk_mode != 0)
-    DevBuf bk_tasks, bk_begins;
-    int bk_ntask = 0;
-    long long bk_nblocks = 0;
-    // tasks of the tcgen05 kernel for 32 < D <= 64
-    DevBuf t64_tasks, t64_begins;
-    int t64_ntask = 0;
-    long long t64_nblocks = 0;
-    size_t tc_smem = 0;
-  };
-  std::vector<Level> levels;
-  DevBuf gram_tasks, gram_begins, msg_tasks, sum_tasks, cond;
-  int gram_ntask = 0, nmsg = 0, nsum = 0;
-  long long gram_nblocks = 0;
-  // Gram tasks of the tcgen05 kernels (one CTA per chunk): C <= 32, 32 < C <= 64
-  DevBuf gtc_tasks, gtc_begins, g64_tasks, g64_begins;
-  int gtc_ntask = 0, g64_ntask = 0;
-  long long gtc_nblocks = 0, g64_nblocks = 0;
+  DevBuf arena, cond;
+  std::vector<SweepLaunch> launches;
   int nkernels = 0;
   cudaGraphExec_t graph = nullptr;
   SweepBatch() = default;
@@ -113,16 +109,17 @@ struct SweepBatch {
   SweepBatch& operator=(SweepBatch&& o) noexcept;
   ~SweepBatch() { reset_graph(); }
   void reset_graph();
-  uint64_t bytes() const;
+  uint64_t bytes() const { return arena.bytes + cond.bytes; }
 };
 
 struct SweepPlan {
   bool valid = false;
   DevBuf partial, dist;
-  std::vector<LevelHost> levels;
+  std::vector<WaveHost> waves;
   std::vector<GramTask> gram;
-  std::vector<long long> gram_blocks;  // blocks of each gram task
-  std::vector<MsgTask> msg[2];
+  std::vector<long long> gram_blocks;  // blocks of each gram task (CUDA-core kernel)
+  std::vector<LegGramTask> lg[2];      // fused last absorption + Gram, per parity
+  std::vector<MsgTask> msg[2];         // one per target, per message-arena parity
   SweepBatch single[2];
   double flops = 0.0, bytes_alg = 0.0;
   SweepPlan() = default;
@@ -144,8 +141,11 @@ double effective_tol(int prec, double tol);
 bool stop_on_growth(int prec, double prev, double c);
 inline bool reduced_sweeps(int prec) { return prec != TNBP_C128; }
 void prepare_kernels(int prec);
+size_t wave_budget_bytes();
+bool autotune_enabled();
 bool tcgen05_enabled();
 bool bulk_leg_enabled();
+bool leg_gram_enabled();
 int num_sms();
 void check_tc_error(cudaStream_t stream);
 
@@ -215,6 +215,9 @@ struct Job {
   int cur = 0;
   int last_par = 0;
   SweepPlan plan;
+  uint64_t plan_serial = 0;  // unique per plan build (keys of the server's sweep graphs)
+  size_t wave_budget = 0;    // wave byte budget of the next plan (0: one wave)
+  bool tuning = false;       // the autotuner sets wave_budget itself
   long long sweeps_run = 0;
   float last_sweep_ms = 0.f;
   double total_sweep_ms = 0.0, total_sweep_flops = 0.0, total_sweep_bytes = 0.0;
@@ -240,6 +243,9 @@ struct Job {
   void bp_sweep();
   double bp_condition();
   void bp_run(double tol, int max_iter, int* iters, double* cond);
+  std::string tune_key() const;
+  void choose_wave_budget();
+  void autotune_waves();
   void absorb_tpo(const Tpo& tpo);
   void run_chains(std::vector<ChainEntry>& chains);
   void truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_out);

@@ -207,6 +207,24 @@ __global__ void __launch_bounds__(kThreads) k_gram(const GramTask* __restrict__ 
   }
 }
 
+// Fused last leg absorption + message Gram (tc_leg_gram.cuh):
+//   N_t[c, c'] = sum_{o, j'} (sum_j X[c, j, o] E_w[j, j']) conj(V[c', j', o]).
+struct LegGramTask {
+  const void* X;         // complex64, same layout as V
+  const void* V;         // complex64 site tensor
+  const void* E;         // Dw x Dw message on leg w (element type MR)
+  long long st, sw;      // element strides of legs t and w
+  long long L1, Mid;     // outer index o = a + L1 (b + Mid c)
+  long long s_mid, s_r;  // element offset of o = a + s_mid b + s_r c
+  long long n_outer;     // number of outer indices
+  int Dt, Dw;
+  int mode;              // thread order: 0 c fastest, 1 j fastest, 2 o fastest
+  int chunk_tiles;       // tiles of 4 outer indices per CTA
+  int nchunk;
+  double2* partial;      // [nchunk][Dt * Dt], N[c + Dt c']
+  long long block_begin; // exclusive prefix of nchunk over tasks
+};
+
 // ---------------------------------------------------------------------------
 // Reduce Gram partials (fixed order), normalize by the Frobenius norm
 // (bp.h:166), store the new message, and the distance to the normalized

@@ -50,7 +50,7 @@ Server::Server(int precision, uint64_t budget_bytes, int max_active_jobs)
 }
 
 Server::~Server() {
-  batch = SweepBatch();
+  sweeps.clear();
   for (auto& kv : reqs) { kv.second->job.reset(); kv.second->tpos.reset(); }
   tpo_cache.clear();
   if (hcond) cudaFreeHost(hcond);
@@ -67,8 +67,8 @@ static int sweep_slots(int g) {
 
 // Peak device bytes of a job on `edges` whose BP runs at bond dimension
 // D[e] on edge e (physical dimension 2): per site the tensor, its spare
-// buffer, the two chain buffers of truncation, the complex64 sweep copy
-// (TNBP_MIXED) and the sweep scratch slots of its degree; both message arenas
+// buffer, the two chain buffers of truncation and the complex64 sweep copy
+// (TNBP_MIXED); the sweep scratch slots of the largest wave; both message arenas
 // twice; per-edge truncation work and Gram partials; plus extra_bytes; 10 %
 // and 8 MiB of margin.
 uint64_t footprint_estimate(const std::vector<std::pair<int, int>>& edges, const std::vector<double>& D, int prec,
@@ -87,9 +87,16 @@ uint64_t footprint_estimate(const std::vector<std::pair<int, int>>& edges, const
       n[pos[v]] *= D[e];
       ++deg[pos[v]];
     }
-  double bytes = 0.0;
-  for (size_t i = 0; i < sites.size(); ++i)
-    bytes += n[i] * (4.0 * esz + shadow + wsz * sweep_slots(deg[i]));  // V, spare, 2 chain buffers
+  double bytes = 0.0, slots_all = 0.0, unit_max = 0.0;
+  for (size_t i = 0; i < sites.size(); ++i) {
+    bytes += n[i] * (4.0 * esz + shadow);  // V, spare, 2 chain buffers, sweep copy
+    slots_all += n[i] * wsz * sweep_slots(deg[i]);
+    unit_max = std::max(unit_max, n[i] * wsz * std::max(1, deg[i]));
+  }
+  // sweep scratch: one wave's units at a time (a wave stays within the wave
+  // budget unless it is a single unit), all of them without a budget
+  const double wave = (double)wave_budget_bytes();
+  bytes += wave > 0.0 ? std::min(slots_all, std::max(wave, unit_max)) : slots_all;
   for (size_t e = 0; e < ne; ++e) {
     const double dd = D[e] * D[e];
     bytes += 4.0 * 2.0 * dd * esz;   // message arenas (old + new)
@@ -285,8 +292,47 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
       if (!r->job->plan.valid) r->job->build_plan();
     }
     prepare_kernels(prec);
-    build_batch(entries, batch, stream);
-    note_launch(launch_batch(batch, prec, stream));
+    std::vector<uint64_t> key;
+    for (auto& e : entries) key.push_back(2 * e.job->plan_serial + (uint64_t)e.parity);
+    auto it = sweeps.find(key);
+    if (it == sweeps.end()) {
+      auto cs = std::make_unique<CachedSweep>();
+      build_batch(entries, cs->batch, stream);
+      it = sweeps.emplace(key, std::move(cs)).first;
+      sweeps_lru.push_back(key);
+      while (sweeps.size() > sweeps_cap) {
+        sweeps.erase(sweeps_lru.front());
+        sweeps_lru.pop_front();
+      }
+    } else {
+      sweeps_lru.remove(key);
+      sweeps_lru.push_back(key);
+    }
+    CachedSweep& cs = *it->second;
+    SweepBatch& batch = cs.batch;
+    if (cs.uses == 1 && !batch.graph) {
+      TNBP_TRACE_SCOPE("server.3_graph_capture");
+      cudaGraph_t graph;
+      CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        batch.nkernels = launch_batch(batch, prec, stream);
+      } catch (...) {
+        cudaStreamEndCapture(stream, &graph);
+        throw;
+      }
+      CK(cudaStreamEndCapture(stream, &graph));
+      CK(cudaGraphInstantiate(&batch.graph, graph, 0));
+      cudaGraphDestroy(graph);
+    }
+    if (batch.graph) {
+      CK(cudaGraphLaunch(batch.graph, stream));
+      note_launch(batch.nkernels);
+      ++graph_launches;
+    } else {
+      note_launch(launch_batch(batch, prec, stream));
+      ++eager_launches;
+    }
+    ++cs.uses;
     if (hcond_cap < entries.size()) {
       if (hcond) cudaFreeHost(hcond);
       hcond_cap = std::max<size_t>(64, 2 * entries.size());

@@ -63,7 +63,19 @@ struct Server {
   std::map<int64_t, std::unique_ptr<Request>> reqs;
   std::vector<int64_t> active;
   uint64_t in_use = 0;
-  SweepBatch batch;
+  // Batched sweeps by membership: key = (plan serial, parity) of every job
+  // in the batch.  A batch seen for the first time is launched kernel by
+  // kernel; seen again (the same jobs, e.g. two steps later with the same
+  // parities) it is captured as a CUDA graph and from then on relaunched as
+  // one graph.  Least recently used entries are dropped beyond the cap.
+  struct CachedSweep {
+    SweepBatch batch;
+    int uses = 0;
+  };
+  std::map<std::vector<uint64_t>, std::unique_ptr<CachedSweep>> sweeps;
+  std::list<std::vector<uint64_t>> sweeps_lru;
+  size_t sweeps_cap = 16;
+  int64_t graph_launches = 0, eager_launches = 0;
   // TPO cache keyed by the circuit (and its TPO options), least recently
   // used evicted first; requests keep their set alive after eviction
   std::map<std::string, std::shared_ptr<const TpoSet>> tpo_cache;
