@@ -30,6 +30,7 @@ import argparse
 import json
 import math
 import os
+import re
 import subprocess
 import sys
 import tempfile
@@ -56,6 +57,17 @@ CPU_SAMPLE_STEPS = 5  # Floquet steps of the CPU reference sample
 # work, so the bench serves its first SERVED_N requests (a prefix of the same
 # seeded stream; --served-requests changes it).
 SERVED_SEED, SERVED_TOTAL, SERVED_N = 25, 512, 8
+
+
+METRIC = "estimator solves/s (mixed path; plain FP64 GPU path and |dE| beside)"
+
+
+def workload_config(theta_h, world):
+    return {"workload": f"kicked-Ising {L_SIDE}x{L_SIDE} open PEPS, {STEPS} steps, chi={CHI}, RZZ(-pi/4), RX(theta_h)",
+            "theta_h": theta_h, "seed": SEED, "bp_tol": BP_TOL, "bp_max_iter": BP_MAXIT,
+            "sv_min": SV_MIN, "observable": f"(1/{L_SIDE * L_SIDE}) sum Z_i + 32 NN ZZ",
+            "parallelism": f"replicas x{world}",
+            "l2": "no flush: site tensors at BP time (~3 GB) exceed the 126 MB L2"}
 
 
 def workload(seed=SEED):
@@ -137,11 +149,14 @@ def random_circuit_workload(seed=SEED, L=10, layers=12):
     return "\n".join(out) + "\n", random_observable(rng, n, 64)
 
 
-def estimator_from_qasm(tb, precision, qasm, pauli, chi, clusters=None):
+def estimator_from_qasm(tb, precision, qasm, pauli, chi, clusters=None, per_term=None):
     """QasmToTPO layers, then the estimator loop; returns (sum, terms kept,
     terms dropped).  With a dict `clusters`, every row of the observable is
     also measured (the dropped ones on their tree clusters) into it: the
-    all-terms sum and the host time of that measurement."""
+    all-terms sum and the host time of that measurement.  With a dict
+    `per_term`, the kept terms' values are stored in it in the order the
+    reference app prints them (one-site terms, then two-site terms, each in
+    file order)."""
     edges = tb.EdgesFromQasm(qasm)
     layers = tb.QasmToTPO(qasm, edges)
     terms = tb.load_sparse_pauli(pauli, edges)
@@ -150,7 +165,11 @@ def estimator_from_qasm(tb, precision, qasm, pauli, chi, clusters=None):
             tb.AbsorbTPO(st, layer)
             tb.BeliefPropagationLoop(st, BP_TOL, BP_MAXIT)
             tb.Truncation(st, chi, SV_MIN)
-        total, _ = tb.MeasurePauliSum(st, terms)
+        total, per = tb.MeasurePauliSum(st, terms)
+        if per_term is not None:
+            kinds = np.asarray(terms.kind)
+            per_term["one"] = [float(v.real) for v in per[kinds == 1]]
+            per_term["two"] = [float(v.real) for v in per[kinds == 2]]
         if clusters is not None:
             t = time.perf_counter()
             all_sum, vals, kinds = tb.MeasurePauliText(st, pauli, clusters=True)
@@ -335,21 +354,19 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def solve(tb, precision, theta_h, pauli_text, resident=None, events=None):
-    """One estimator solve.  Returns (sum, per-solve stats).  With `resident`
-    the state and TPO were created beforehand (device-resident inputs)."""
+def solve(tb, precision, theta_h, pauli_text, events=None):
+    """One estimator solve from host data.  Returns (sum, per-solve stats).
+    With `events`, a CUDA event is recorded once the state and TPO are on the
+    device (the start of the resident-input timing)."""
     import torch
     h2d = d2h = 0
-    if resident is None:
-        edges = tb.bond_square_lattice(L_SIDE, L_SIDE)
-        layer = tb.KickedIsingTPO(edges, THETA_J / 2, 0.0, theta_h / 2, 1.0)
-        st = tb.State(edges, precision)
-        tpo = st.tpo(layer)
-        terms = tb.load_sparse_pauli(pauli_text, edges)
-        h2d += len(edges) * 8 + layer.op_data.nbytes + layer.edge_rank.nbytes + layer.op_offset.nbytes
-        h2d += len(terms) * (4 * 3 + 2 + 16)
-    else:
-        st, tpo, terms = resident
+    edges = tb.bond_square_lattice(L_SIDE, L_SIDE)
+    layer = tb.KickedIsingTPO(edges, THETA_J / 2, 0.0, theta_h / 2, 1.0)
+    st = tb.State(edges, precision)
+    tpo = st.tpo(layer)
+    terms = tb.load_sparse_pauli(pauli_text, edges)
+    h2d += len(edges) * 8 + layer.op_data.nbytes + layer.edge_rank.nbytes + layer.op_offset.nbytes
+    h2d += len(terms) * (4 * 3 + 2 + 16)
     if events is not None:
         torch.cuda.synchronize()
         events.append(torch.cuda.Event(enable_timing=True))
@@ -397,11 +414,6 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local_rank))
     theta_h, pauli_text = workload()
     edges = tb.bond_square_lattice(L_SIDE, L_SIDE)
-
-    def make_resident(prec):
-        layer = tb.KickedIsingTPO(edges, THETA_J / 2, 0.0, theta_h / 2, 1.0)
-        st = tb.State(edges, prec)
-        return st, st.tpo(layer), tb.load_sparse_pauli(pauli_text, edges)
 
     # warm-up (untimed): same work as a timed step
     for _ in range(args.warmup):
@@ -461,7 +473,7 @@ def run_ours(args, rank, world, local_rank):
         except (OSError, ValueError):
             traffic = None
     line = {
-        "metric": "estimator solves/s (mixed path; plain FP64 GPU path and |dE| beside)",
+        "metric": METRIC,
         "value": value,
         "unit": "solves/s",
         "n_gpus": world,
@@ -474,12 +486,7 @@ def run_ours(args, rank, world, local_rank):
         "dtype": "mixed: c64 BP sweeps (3xTF32 / FP32 products, FP64 sums) on a c128 state; FP64 absorb, "
                  "truncation, measurement",
         "data": "synthetic (seeded kicked-Ising circuit and Pauli observable)",
-        "config": {"workload": f"kicked-Ising {L_SIDE}x{L_SIDE} open PEPS, {STEPS} steps, chi={CHI}, "
-                               "RZZ(-pi/4), RX(theta_h)",
-                   "theta_h": theta_h, "seed": SEED, "bp_tol": BP_TOL, "bp_max_iter": BP_MAXIT,
-                   "sv_min": SV_MIN, "observable": "(1/256) sum Z_i + 32 NN ZZ",
-                   "parallelism": f"replicas x{world}",
-                   "l2": "no flush: site tensors at BP time (~3 GB) exceed the 126 MB L2"},
+        "config": workload_config(theta_h, world),
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": stats[-1]["h2d"],
                 "d2h_bytes_per_step": stats[-1]["d2h"]},
         "gpu_launches": int(launches),
@@ -533,23 +540,51 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_fp64:
         line["random_circuit"] = random_circuit_summary(tb)
     if world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_sample(theta_h)
+        # the reference CPU solve and the GPU solves of the same prefix of
+        # the workload, timed in this run (apples to apples)
+        ref_vals, vm, vp = {}, {}, {}
+        cpu_s = cpu_sample(theta_h, values=ref_vals)
+        gm, sm = gpu_prefix_solve(tb, tb.MIXED, theta_h, pauli_text, per_term=vm)
+        gp, sp = gpu_prefix_solve(tb, tb.C128, theta_h, pauli_text, per_term=vp)
+
+        def term_diff(got):
+            if not ref_vals or len(got.get("one", [])) != len(ref_vals["one"]) or \
+                    len(got.get("two", [])) != len(ref_vals["two"]):
+                return None
+            d = [abs(a - b) for a, b in zip(got["one"] + got["two"], ref_vals["one"] + ref_vals["two"])]
+            return max(d) if d else 0.0
+        if cpu_s is not None:
+            line["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "solves/s", "cores": os.cpu_count(),
+                                    "kind": "reference", "seconds": cpu_s, "sample": prefix_sample_text()}
+        line["cpu_matched"] = {
+            "sample": prefix_sample_text(),
+            "cpu_reference_s": cpu_s, "gpu_mixed_s": gm, "gpu_plain_fp64_s": gp,
+            "speedup_mixed": (cpu_s / gm) if cpu_s else None,
+            "speedup_plain_fp64": (cpu_s / gp) if cpu_s else None,
+            "dE_mixed_vs_plain": abs(sm - sp),
+            # the reference app's printed per-term values (16 digits) against
+            # the GPU paths' on the same prefix
+            "parity_vs_reference": {"terms": len(ref_vals.get("one", [])) + len(ref_vals.get("two", [])),
+                                    "max_dterm_plain_fp64": term_diff(vp), "max_dterm_mixed": term_diff(vm)},
+            "note": "GPU times through the public API from QASM text (host wall clock, includes TPO build)"}
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
 
 
-def cpu_sample(theta_h, steps=CPU_SAMPLE_STEPS):
-    """The reference's estimator app (oracle/_ref/estimator: unchanged tnbp
-    headers and app on the project's CPU tensor backend, OpenMP threads = all
-    host cores) on the first `steps` Floquet steps of the same workload.
-    value = (steps / 20) / seconds: each sampled Floquet step counted as 1/20
-    of a solve.  The sampled steps run BP at bond dimension <= 16; the later
-    steps at 32 cost far more, so this over-states the CPU's solves/s."""
+def cpu_sample(theta_h, steps=CPU_SAMPLE_STEPS, values=None):
+    """One complete solve of the reference's estimator app
+    (oracle/_ref/estimator: the unchanged tnbp estimator app and headers on
+    the project's CPU tensor backend, OpenMP threads = all host cores) on the
+    first `steps` Floquet steps of the same workload (same lattice, angles,
+    chi, tolerances and observable; BP at bond dimension <= 16): QASM read,
+    TPO built, every step's absorb / BP / truncation, then the Pauli terms.
+    Returns the measured wall time of that solve; nothing is extrapolated.
+    With a dict `values`, the per-term values the app printed are stored in
+    it (keys "one" and "two")."""
     exe = os.path.join(ROOT, "oracle", "_ref", "estimator")
     if not os.path.exists(exe):
-        return {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "reference",
-                "sample": "oracle/_ref/estimator not built"}
+        return None
     _, pauli_text = workload()
     d = tempfile.mkdtemp()
     qp, pp = os.path.join(d, "c.qasm"), os.path.join(d, "p.txt")
@@ -557,38 +592,62 @@ def cpu_sample(theta_h, steps=CPU_SAMPLE_STEPS):
     open(pp, "w").write(pauli_text)
     env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count()))
     t = time.perf_counter()
-    subprocess.run([exe, "--circuit", qp, "--sparse_pauli", pp, "--max_bond_dim", str(CHI), "--bp_tolerance",
-                    repr(BP_TOL), "--max_bp_iterations", str(BP_MAXIT), "--sv_min", repr(SV_MIN)],
-                   check=True, capture_output=True, env=env, timeout=1800)
+    r = subprocess.run([exe, "--circuit", qp, "--sparse_pauli", pp, "--max_bond_dim", str(CHI), "--bp_tolerance",
+                        repr(BP_TOL), "--max_bp_iterations", str(BP_MAXIT), "--sv_min", repr(SV_MIN)],
+                       check=True, capture_output=True, env=env, timeout=1800, text=True)
     dt = time.perf_counter() - t
-    return {"value": (steps / STEPS) / dt, "unit": "solves/s", "cores": os.cpu_count(), "kind": "reference",
-            "seconds": dt,
-            "sample": f"first {steps} of {STEPS} Floquet steps of the same solve (BP at D<=16), "
-                      f"counted as {steps}/{STEPS} of a solve; later steps (D=32) cost ~30x more, "
-                      "so this over-states CPU solves/s"}
+    if values is not None:
+        values["one"] = [float(v) for v in re.findall(r"single site operator at site \d+ (\S+)", r.stdout)]
+        values["two"] = [float(v) for v in re.findall(r"two site operator at sites \(\d+,\d+\) (\S+)", r.stdout)]
+    return dt
+
+
+def prefix_sample_text(steps=CPU_SAMPLE_STEPS):
+    return (f"one complete estimator solve of the first {steps} of the {STEPS} Floquet steps of this workload "
+            f"(same lattice, angles, chi, tolerances and observable; BP at bond dimension <= 16), wall clock; "
+            f"value = those prefix solves per second, measured, not extrapolated to the {STEPS}-step solve")
+
+
+def gpu_prefix_solve(tb, precision, theta_h, pauli_text, steps=CPU_SAMPLE_STEPS, per_term=None):
+    """The same prefix solve as cpu_sample through the public API on the GPU
+    (QASM text in, estimator loop, Pauli sum out), host wall clock."""
+    import torch
+    qasm = kicked_ising_qasm(steps, THETA_J, theta_h)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    total, _, _ = estimator_from_qasm(tb, precision, qasm, pauli_text, CHI, per_term=per_term)
+    torch.cuda.synchronize()
+    return time.perf_counter() - t, total
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
     theta_h, _ = workload()
-    vals = []
+    exe = os.path.join(ROOT, "oracle", "_ref", "estimator")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/estimator is not built (build() compiles "
+                                                              "it from the reference tree)"}))
+        return
     for _ in range(args.warmup):
         cpu_sample(theta_h)
+    times = []
+    t_all = time.perf_counter()
     for _ in range(args.steps):
-        vals.append(cpu_sample(theta_h))
-    v = [x["value"] for x in vals if x["value"]]
-    value = float(np.mean(v)) if v else None
+        times.append(cpu_sample(theta_h))
+    wall = time.perf_counter() - t_all
+    value = len(times) / sum(times)
     line = {
         "impl": "reference",
-        "metric": "estimator solves/s (mixed path; plain FP64 GPU path and |dE| beside)",
+        "metric": METRIC,
         "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": (1e3 / value) if value else None, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded kicked-Ising circuit and Pauli observable)",
-        "config": {"workload": "kicked-Ising 16x16 open PEPS, 20 steps, chi=16, RZZ(-pi/4), RX(theta_h)",
-                   "theta_h": theta_h, "seed": SEED},
+        "config": workload_config(theta_h, world),
+        "sample": prefix_sample_text(),
+        "wall_s": wall,
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": os.cpu_count(), "kind": "reference",
-                         "sample": vals[-1]["sample"] if vals else None},
+                         "sample": prefix_sample_text()},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
