@@ -28,6 +28,9 @@ oracle/_ref/, and this script runs them on seeded synthetic inputs:
                      values it printed after a second pass loaded from it
   config1.json       observables of the 4x4 kicked-Ising workload from the
                      reference apps kicked_ising_lattice and estimator
+  est_rc10x10.json   the estimator app's printed values on the benchmark's
+                     random-circuit workload at full size (10x10, 12 U3 + CZ
+                     layers, chi 32, 64-term observable; --only est_rc10)
 
 usage: python tests/golden/make_golden.py [--ref <reference tree>]   (default: $TNBP_REFERENCE)
 Needs the reference sources (only in the build container); the fixtures it
@@ -204,6 +207,28 @@ def run_opt_estimator(name, qasm, pauli, chi, sv_min, tol, maxit, eps):
     with open(os.path.join(HERE, f"opt_{name}.json"), "w") as f:
         json.dump(res, f, indent=1)
     print(f"opt_{name}: {len(one)} one-site, {len(two)} two-site values, conditions {conds}")
+
+
+def run_estimator_values(name, qp, pp, chi, sv_min, tol, maxit):
+    """The reference estimator app on an input pair: every printed value
+    (one- and two-site terms in print order, conditions, bond dims) and the
+    app's wall time."""
+    import time
+    t = time.perf_counter()
+    out = subprocess.check_output(
+        [os.path.join(REF_BIN, "estimator"), "--circuit", qp, "--sparse_pauli", pp, "--max_bond_dim", str(chi),
+         "--bp_tolerance", repr(tol), "--max_bp_iterations", str(maxit), "--sv_min", repr(sv_min)], text=True)
+    dt = time.perf_counter() - t
+    one = [[int(s_), float(v)] for s_, v in re.findall(r"single site operator at site (\d+) (\S+)", out)]
+    two = [[int(a_), int(b_), float(v)] for a_, b_, v in
+           re.findall(r"two site operator at sites \((\d+),(\d+)\) (\S+)", out)]
+    dims = [int(v) for v in re.findall(r"bond dim = (\d+)", out)]
+    conds = [float(v) for v in re.findall(r"condition at step \d+ = (\S+)", out)]
+    res = dict(chi=chi, sv_min=sv_min, tol=tol, maxit=maxit, one=one, two=two, final_bond_dims=dims[-200:],
+               conditions=conds, seconds=dt)
+    with open(os.path.join(HERE, f"est_{name}.json"), "w") as f:
+        json.dump(res, f, indent=1)
+    print(f"est_{name}: {len(one)} one-site, {len(two)} two-site values, {len(conds)} sweeps, {dt:.1f} s")
 
 
 def kicked_ising_no_barrier(Lx, Ly, steps, theta_j, theta_h):
@@ -443,6 +468,17 @@ def main():
             with open(os.path.join(INPUTS, f"rc10x10.{ext}"), "w") as f:
                 f.write(txt)
         run_hostparity("rc10x10", ["qasm", os.path.join(INPUTS, "rc10x10.qasm"), os.path.join(INPUTS, "rc10x10.txt")])
+    if "est_rc10" in jobs:
+        # the benchmark's random-circuit workload at full size through the
+        # reference app (BP at bond dimension <= 8, so the CPU run is short)
+        sys.path.insert(0, ROOT)
+        import bench
+        q, p = bench.random_circuit_workload()
+        for ext, txt in (("qasm", q), ("txt", p)):
+            with open(os.path.join(INPUTS, f"rc10x10.{ext}"), "w") as f:
+                f.write(txt)
+        run_estimator_values("rc10x10", os.path.join(INPUTS, "rc10x10.qasm"), os.path.join(INPUTS, "rc10x10.txt"),
+                             32, bench.SV_MIN, bench.BP_TOL, bench.BP_MAXIT)
     if "opttpo" in jobs:
         q = zz_cx_qasm(3, 3, 2, -0.7, 0.8)  # generic angle: no tie at a rank-1 cut
         qp = os.path.join(INPUTS, "zzcx3x3.qasm")

@@ -116,3 +116,23 @@ def test_estimator_app_with_num_gates(precision, tol):
     assert len(one) == len(ref["one"]) and len(two) == len(ref["two"]), out
     for a, b in zip(one + two, ref["one"] + ref["two"]):
         assert abs(a - b) <= tol, (a, b)
+
+
+@pytest.mark.parametrize("precision,tol", [("c128", 1e-10), ("mixed", 1e-6)])
+def test_estimator_app_full_size_random_circuit(precision, tol):
+    """The benchmark's random-circuit workload at full size (10x10 qubits, 12
+    layers of U3 on every qubit and CZ on one edge colouring, chi 32, the
+    64-term observable): every value the reference estimator app printed
+    (tests/golden/est_rc10x10.json, made by make_golden.py --only est_rc10)
+    against the engine's app on the same files and flags."""
+    import json
+    ref = json.load(open(os.path.join(HERE, "golden", "est_rc10x10.json")))
+    one, two, out = _run("rc10x10", ref, precision)
+    got_one = [(int(m.group(1)), float(m.group(2))) for m in ONE.finditer(out)]
+    assert [s for s, _ in got_one] == [s for s, _ in ref["one"]], out
+    for (_, a), (_, b) in zip(got_one, ref["one"]):
+        assert abs(a - b) <= tol, (a, b)
+    got_two = [(int(m.group(1)), int(m.group(2)), float(m.group(3))) for m in TWO.finditer(out)]
+    assert [(a, b) for a, b, _ in got_two[: len(ref["two"])]] == [(a, b) for a, b, _ in ref["two"]]
+    for (_, _, a), (_, _, b) in zip(got_two, ref["two"]):
+        assert abs(a - b) <= tol, (a, b)
