@@ -78,6 +78,39 @@ def build(verbose=True, jobs=4):
     return LIB
 
 
+DROPIN_DIR = os.path.join(HERE, "apps", "_dropin")
+DROPIN_INC = os.path.join(INCLUDE, "tnbp_dropin")
+DROPIN_SRC = os.path.join(HERE, "dropin", "device_overloads.cpp")
+# (app, C++ standard): the reference's own app sources, compiled unchanged
+DROPIN_APPS = (("estimator", "c++17"), ("kicked_ising_lattice", "c++20"))
+
+
+def build_dropin(ref, verbose=True):
+    """Compile tnbp's apps (apps/estimator, apps/kicked_ising_lattice) from
+    the reference tree `ref`, unchanged, against this library: the tensor
+    backend header include/tnbp_dropin/gqten/gqten.h (first on the include
+    path) and the GPU overloads of tnbp's hot-path functions
+    (tnbp_b200/dropin/device_overloads.cpp), linked to libtnbp_b200.so.  The
+    binaries go to tnbp_b200/apps/_dropin/.  Needs the reference sources,
+    which only the build machine has; the binaries travel with the tree."""
+    os.makedirs(DROPIN_DIR, exist_ok=True)
+    deps = [DROPIN_SRC, LIB, os.path.join(DROPIN_INC, "gqten", "gqten.h"), os.path.join(DROPIN_INC, "mpi.h"),
+            os.path.join(INCLUDE, "tnbp_b200.h")]
+    for app, std in DROPIN_APPS:
+        src = os.path.join(ref, "apps", app, "main.cc")
+        out = os.path.join(DROPIN_DIR, app)
+        if not os.path.exists(src):
+            continue
+        if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(p) for p in deps + [src]):
+            continue
+        cmd = ["g++", f"-std={std}", "-O2", "-I", DROPIN_INC, "-I", INCLUDE, "-I",
+               os.path.join(ref, "external", "min-tci", "include"), "-I", os.path.join(ref, "include"), src,
+               DROPIN_SRC, "-L", HERE, "-ltnbp_b200", "-Wl,-rpath,$ORIGIN/../..", "-o", out]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
+
+
 if __name__ == "__main__":
     build()
     sys.exit(0)
