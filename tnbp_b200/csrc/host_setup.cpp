@@ -10,7 +10,9 @@
 
 #include <algorithm>
 #include <cctype>
+#include <climits>
 #include <cmath>
+#include <cstdint>
 #include <complex>
 #include <cstdlib>
 #include <map>
@@ -179,8 +181,15 @@ static std::vector<cd> gate_matrix(const Instruction& in) {
       return m;
     }
     case Op::CSWAP: {
+      // Fredkin, control q0: swaps q1 and q2 (|011> <-> |101>, indices 3 and
+      // 5); the other six basis states stay.  The reference's table
+      // (qasmtotpo.h:127-137) places the diagonal entry of index 4 at index
+      // 5, which is not unitary; its three-qubit branch cannot run anyway
+      // (it indexes past its path vector), so the correct gate is used here.
       std::vector<cd> m(64, 0.0);
-      m[0] = 1; m[9] = 1; m[18] = 1; m[45] = 1; m[54] = 1; m[63] = 1; m[3 * 8 + 5] = 1; m[5 * 8 + 3] = 1;
+      for (int i : {0, 1, 2, 4, 6, 7}) m[i * 8 + i] = 1;
+      m[3 * 8 + 5] = 1;
+      m[5 * 8 + 3] = 1;
       return m;
     }
     default:
@@ -414,6 +423,107 @@ struct LayerBuilder {
       }
     }
   }
+  // Identity on the physical leg, passing a bond of dimension k from the
+  // site's leg toward `prev` to its leg toward `next` (a path's inner site).
+  void pass_through(int si, int prev, int next, int k) {
+    std::vector<cd> X(k * k * 4, 0.0);
+    for (int x = 0; x < k; ++x)
+      for (int o = 0; o < 2; ++o) X[x + k * x + k * k * (o + 2 * o)] = 1.0;
+    const int lm = leg_toward(si, prev), lp = leg_toward(si, next);
+    attach(ops[si], {std::min(lm, lp), std::max(lm, lp)}, {k, k}, X);
+  }
+  // Three-qubit gate (ccx, cswap; the reference's branch is
+  // qasmtotpo.h:439-698): two operator-Schmidt splits of the 8 x 8 gate,
+  // each a truncated SVD (chi_max 4, s_min 1e-12, sqrt(s) to both sides):
+  //   G[(a), (b), (c)] = sum_{k1,k2} A[k1, a] Bm[k1, k2, b] C[k2, c]
+  // with a = (in, out) of the first qubit of the chosen order, etc.  The
+  // middle qubit is the one with the shortest total distance to the other
+  // two (the instruction's second qubit on ties); bond k1 runs along the
+  // shortest path from the first qubit to the middle one and k2 from the
+  // middle one to the last, through identity pass-through tensors.  Where
+  // the two paths share an edge, that edge carries both bonds (merged in
+  // the same order at both ends), so any three connected qubits work.
+  void three_qubit(const std::vector<int>& q, const std::vector<cd>& U) {
+    int mid = 1;
+    size_t best = SIZE_MAX;
+    for (int m : {1, 0, 2}) {
+      size_t len = 0;
+      for (int o = 0; o < 3; ++o)
+        if (o != m) {
+          const auto p = shortest_path(edges, q[o], q[m]);
+          if (p.size() < 2) throw HostError(-1, "three-qubit gate between disconnected or equal qubits");
+          len += p.size();
+        }
+      if (len < best) { best = len; mid = m; }
+    }
+    int order[3] = {0, mid, 0};
+    {
+      int j = 0;
+      int rest[2];
+      for (int o = 0; o < 3; ++o) if (o != mid) rest[j++] = o;
+      order[0] = rest[0];
+      order[2] = rest[1];
+    }
+    // G[(a_in, a_out), (b_in, b_out), (c_in, c_out)], qubit x = q[order[x]]
+    std::vector<cd> G(64);
+    int bit[3];
+    for (int x = 0; x < 3; ++x) bit[x] = order[x];  // bit position of x in U's index
+    for (int ai = 0; ai < 2; ++ai) for (int ao = 0; ao < 2; ++ao)
+      for (int bi = 0; bi < 2; ++bi) for (int bo = 0; bo < 2; ++bo)
+        for (int ci = 0; ci < 2; ++ci) for (int co = 0; co < 2; ++co) {
+          const int in = (ai << bit[0]) | (bi << bit[1]) | (ci << bit[2]);
+          const int out = (ao << bit[0]) | (bo << bit[1]) | (co << bit[2]);
+          G[(ai + 2 * ao) + 4 * (bi + 2 * bo) + 16 * (ci + 2 * co)] = U[out * 8 + in];
+        }
+    auto keep_of = [](const std::vector<double>& s) {
+      int k = 0;
+      while (k < (int)s.size() && k < 4 && s[k] > 1e-12) ++k;
+      return k == 0 ? 1 : k;
+    };
+    // split 1: (a) x (b, c)
+    std::vector<cd> U1, V1;
+    std::vector<double> s1;
+    small_svd(4, 16, G, U1, s1, V1);
+    const int k1 = keep_of(s1);
+    std::vector<cd> A(k1 * 4), R1(k1 * 16);  // A[k1 + k1 a]; R1[(k1, b), c] as (4 k1) x 4
+    for (int c = 0; c < k1; ++c) {
+      const double sq = std::sqrt(std::abs(s1[c]));
+      for (int a = 0; a < 4; ++a) A[c + k1 * a] = U1[a + 4 * c] * sq;
+      for (int bc = 0; bc < 16; ++bc) {
+        const int b = bc % 4, cc = bc / 4;
+        R1[(c + k1 * b) + 4 * k1 * cc] = sq * V1[c + std::min(4, 16) * bc];
+      }
+    }
+    // split 2: (k1, b) x (c)
+    std::vector<cd> U2, V2;
+    std::vector<double> s2;
+    small_svd(4 * k1, 4, R1, U2, s2, V2);
+    const int k2 = keep_of(s2);
+    const int r2 = std::min(4 * k1, 4);  // rank count of the second SVD
+    std::vector<cd> Bm(k1 * k2 * 4), C(k2 * 4);  // Bm[x1 + k1 x2 + k1 k2 b]; C[x2 + k2 c]
+    for (int c = 0; c < k2; ++c) {
+      const double sq = std::sqrt(std::abs(s2[c]));
+      for (int x1 = 0; x1 < k1; ++x1)
+        for (int b = 0; b < 4; ++b) Bm[x1 + k1 * c + k1 * k2 * b] = U2[(x1 + k1 * b) + 4 * k1 * c] * sq;
+      for (int cc = 0; cc < 4; ++cc) C[c + k2 * cc] = sq * V2[c + r2 * cc];
+    }
+    const int qa = q[order[0]], qb = q[order[1]], qc = q[order[2]];
+    const auto p1 = shortest_path(edges, qa, qb), p2 = shortest_path(edges, qb, qc);
+    // bond k1 from qa to qb
+    attach(ops[site_index(qa)], {leg_toward(site_index(qa), p1[1])}, {k1}, A);
+    for (size_t i = 1; i + 1 < p1.size(); ++i) pass_through(site_index(p1[i]), p1[i - 1], p1[i + 1], k1);
+    // the middle factor joins both bonds
+    {
+      const int si = site_index(qb);
+      const int la = leg_toward(si, p1[p1.size() - 2]), lc = leg_toward(si, p2[1]);
+      // both bonds leave through the same edge: one merged index x1 + k1 x2
+      // (Bm's layout already), the order of the merges at the other end
+      if (la == lc) attach(ops[si], {la}, {k1 * k2}, Bm);
+      else attach(ops[si], {la, lc}, {k1, k2}, Bm);
+    }
+    for (size_t i = 1; i + 1 < p2.size(); ++i) pass_through(site_index(p2[i]), p2[i - 1], p2[i + 1], k2);
+    attach(ops[site_index(qc)], {leg_toward(site_index(qc), p2[p2.size() - 2])}, {k2}, C);
+  }
   void append(const Instruction& in) {
     // the reference builds NaN operators from an infinite angle (strtod of
     // "1e400") without complaint; here the layer is refused before it can
@@ -424,7 +534,8 @@ struct LayerBuilder {
     const int nq = qubit_count(in);
     if (nq == 1) one_qubit((int)in.qubits[0].index, U);
     else if (nq == 2) two_qubit((int)in.qubits[0].index, (int)in.qubits[1].index, U);
-    else throw HostError(-6, "three-qubit gates are not supported on the estimator path");
+    else if (nq == 3) three_qubit({(int)in.qubits[0].index, (int)in.qubits[1].index, (int)in.qubits[2].index}, U);
+    else throw HostError(-6, "gates on more than three qubits are not supported on the estimator path");
   }
 };
 
