@@ -205,6 +205,20 @@ def random_circuit_summary(tb):
                         "note": "terms the reference drops measured on tree clusters (not in the reference)"}
     res["workload"] = ("random circuit 10x10, 12 layers U3 + CZ (4 colourings, cyclic), chi 32, "
                        "64-term observable (the reference drops >2-qubit and non-adjacent terms); host wall clock")
+    # host cost of a served QASM request's TPO (built once per program and
+    # cached): QasmToTPO, then OptTPObySVD on every layer, against the mixed
+    # solve it feeds
+    edges = tb.EdgesFromQasm(qasm)
+    t = time.perf_counter()
+    layers = tb.QasmToTPO(qasm, edges)
+    t_tpo = time.perf_counter() - t
+    t = time.perf_counter()
+    for layer in layers:
+        tb.OptTPObySVD(edges, layer, 1e-8)
+    t_opt = time.perf_counter() - t
+    res["host_tpo"] = {"qasm_to_tpo_ms": t_tpo * 1e3, "opt_tpo_by_svd_ms": t_opt * 1e3, "layers": len(layers),
+                       "fraction_of_mixed_solve": (t_tpo + t_opt) * res["mixed"]["solves_per_s"],
+                       "note": "host (one thread); per distinct program, cached by the server"}
     return res
 
 
