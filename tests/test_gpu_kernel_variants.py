@@ -5,8 +5,9 @@ The engine picks the kernel of each task by its shape; three switches, read
 once per process, change that choice: TNBP_LEG_BULK=1 routes the eligible
 complex64 tasks to the bulk-staged tcgen05 kernel (cp.async.bulk tiles),
 TNBP_DISABLE_TCGEN05=1 routes every task to the CUDA-core kernels, and
-TNBP_LEG_GRAM=0 runs each target's last absorption and its Gram as separate
-kernels instead of the fused tcgen05 kernel (k_leg_gram_tc, the default).  Each
+TNBP_LEG_GRAM=1 runs each target's last absorption and its Gram in the fused
+tcgen05 kernel (k_leg_gram_tc) instead of the separate kernels (the
+default).  Each
 variant runs in its own process here, on a 3x3 patch at D = 32 (all three
 tree levels and all tile layouts of the bulk kernel: L = 1, 32, 1024) and on
 uneven dims 2..9, with the message tolerance of the other reduced-precision
@@ -56,8 +57,8 @@ print("WORST", worst)
 """
 
 
-@pytest.mark.parametrize("env", [{"TNBP_LEG_BULK": "1"}, {"TNBP_DISABLE_TCGEN05": "1"}, {"TNBP_LEG_GRAM": "0"}, {}],
-                         ids=["bulk-staged", "cuda-core", "unfused-gram", "default"])
+@pytest.mark.parametrize("env", [{"TNBP_LEG_BULK": "1"}, {"TNBP_DISABLE_TCGEN05": "1"}, {"TNBP_LEG_GRAM": "1"}, {}],
+                         ids=["bulk-staged", "cuda-core", "fused-leg-gram", "default"])
 def test_leg_kernel_variant_matches_oracle(env):
     code = SCRIPT.format(root=ROOT, oracle=os.path.join(ROOT, "oracle"))
     full_env = dict(os.environ)

@@ -170,12 +170,30 @@ int tnbp_pauli_terms(const char* text, const int32_t* edges, int64_t ne, int32_t
   });
 }
 
+// The size query (cap 0) and the fill call that follows it with the same
+// program and edges share one build: the layers of the last call on this
+// thread are kept until a call with other inputs.
+namespace {
+struct LastTpo {
+  std::string src;
+  std::vector<int32_t> edges;
+  std::vector<tnbp_host::Layer> layers;
+};
+thread_local LastTpo g_last_tpo;
+}  // namespace
+
 int tnbp_qasm_tpo(const char* src, const int32_t* edges, int64_t ne, int32_t* edge_rank, int64_t* op_offset,
                   double* op_data, int64_t cap, int32_t* n_layers, int64_t* n_elems) {
   return guard([&] {
     need(src != nullptr, "qasm source is NULL");
     auto e = to_edges(edges, ne);
-    auto layers = tnbp_host::qasm_tpo(tnbp_host::parse_qasm(src), e);
+    std::vector<int32_t> key(edges, edges + 2 * ne);
+    if (g_last_tpo.src != src || g_last_tpo.edges != key) {
+      g_last_tpo.layers = tnbp_host::qasm_tpo(tnbp_host::parse_qasm(src), e);
+      g_last_tpo.src = src;
+      g_last_tpo.edges = std::move(key);
+    }
+    const auto& layers = g_last_tpo.layers;
     if (n_layers) *n_layers = (int32_t)layers.size();
     put_layers(layers, ne, (int64_t)tnbp_host::site_labels(e).size(), edge_rank, op_offset, op_data, cap, n_elems);
   });

@@ -453,14 +453,14 @@ Unit make_unit(int site, int u, const std::vector<PlanOp>& all, const SitePlanne
 // Bytes of site tensors plus intermediate slots one wave may hold; 0 puts
 // every unit of the sweep in one wave.  TNBP_WAVE_MB fixes it for every job
 // (no autotuning); otherwise a job uses the autotuned budget of its shape
-// class (below) or this default, a little under the 126 MB L2, which the
-// slots of the wave being computed share with the site tensors streaming
-// through.
+// class (below) or this default of one wave: on the 16x16 D = 32 sweep one
+// wave measured 25.5 ms against 50.5 ms at 96 MiB (L2-sized waves), whose
+// many small launches cost more than the L2 reuse saves.
 size_t wave_budget_bytes() {
   static const size_t v = [] {
     const char* e = std::getenv("TNBP_WAVE_MB");
     if (e && *e) return (size_t)std::strtoull(e, nullptr, 10) << 20;
-    return size_t(96) << 20;
+    return size_t(0);
   }();
   return v;
 }
@@ -733,9 +733,12 @@ void Job::build_plan() {
         g1.L = L; g1.M = M; g1.D = sh[t]; g1.P = 1; g1.C = sh[t];
         g1.ctiles = (g1.C + kColTile - 1) / kColTile;
         g1.Q = L * M;
-        // chunks of at most Q/128 rows (multiples of 64), so that even a
-        // wave of one unit gives every SM Gram work
-        long long cr = ((g1.Q / 128) + 63) / 64 * 64;
+        // chunks of about Q/16 rows (multiples of 64, 256..4096): FP64
+        // partials of one sweep stay a small fraction of its traffic, and
+        // one wave of all sites gives every SM work; L2-sized waves of one
+        // unit use Q/128 so that each of their Gram launches fills the GPU
+        const long long div = budget ? 128 : 16;
+        long long cr = ((g1.Q / div) + 63) / 64 * 64;
         cr = std::max<long long>(256, std::min<long long>(4096, cr));
         g1.chunk_rows = cr;
         g1.nchunk = (int)((g1.Q + cr - 1) / cr);
@@ -1116,14 +1119,15 @@ bool bulk_leg_enabled() {
   return on;
 }
 
-// The last absorption of every target with dims <= 32 runs fused with its
-// Gram (k_leg_gram_tc) on the reduced-precision paths; TNBP_LEG_GRAM=0
-// returns those targets to the separate leg and Gram kernels (both compute
-// the same contraction; used to compare the two).
+// TNBP_LEG_GRAM=1 runs the last absorption of every target with dims <= 32
+// fused with its Gram (k_leg_gram_tc) on the reduced-precision paths; by
+// default those targets use the separate leg and Gram kernels, which
+// measured faster (16x16 D = 32 sweep in one wave: 25.5 ms separate, 34.7
+// ms fused).  Both compute the same contraction.
 bool leg_gram_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("TNBP_LEG_GRAM");
-    return !(e && e[0] == '0');
+    return e && e[0] == '1';
   }();
   return on;
 }

@@ -351,6 +351,14 @@ struct LayerBuilder {
   std::map<int, int> pos;
   std::vector<std::vector<int>> bonds;  // per site index: incident edge ids
   std::vector<SiteOp> ops;
+  // shortest paths by (from, to) label: FindShortestPath's BFS is the same
+  // for every gate on the pair, so each pair is searched once per builder
+  std::map<std::pair<int, int>, std::vector<int>> paths;
+  const std::vector<int>& path(int a, int b) {
+    auto it = paths.find({a, b});
+    if (it == paths.end()) it = paths.emplace(std::make_pair(a, b), shortest_path(edges, a, b)).first;
+    return it->second;
+  }
   LayerBuilder(const Edges& e) : edges(e) {
     sites = site_labels(e);
     for (size_t i = 0; i < sites.size(); ++i) pos[sites[i]] = (int)i;
@@ -405,7 +413,7 @@ struct LayerBuilder {
         B[c + k * rw] = sq * Vh[c + 4 * rw];
       }
     }
-    const auto path = shortest_path(edges, qa, qb);
+    const auto& path = this->path(qa, qb);
     if (path.size() < 2) throw HostError(-1, "two-qubit gate between disconnected or equal qubits");
     for (size_t i = 0; i < path.size(); ++i) {
       const int si = site_index(path[i]);
@@ -450,7 +458,7 @@ struct LayerBuilder {
       size_t len = 0;
       for (int o = 0; o < 3; ++o)
         if (o != m) {
-          const auto p = shortest_path(edges, q[o], q[m]);
+          const auto& p = path(q[o], q[m]);
           if (p.size() < 2) throw HostError(-1, "three-qubit gate between disconnected or equal qubits");
           len += p.size();
         }
@@ -508,7 +516,8 @@ struct LayerBuilder {
       for (int cc = 0; cc < 4; ++cc) C[c + k2 * cc] = sq * V2[c + r2 * cc];
     }
     const int qa = q[order[0]], qb = q[order[1]], qc = q[order[2]];
-    const auto p1 = shortest_path(edges, qa, qb), p2 = shortest_path(edges, qb, qc);
+    const auto& p1 = path(qa, qb);
+    const auto& p2 = path(qb, qc);
     // bond k1 from qa to qb
     attach(ops[site_index(qa)], {leg_toward(site_index(qa), p1[1])}, {k1}, A);
     for (size_t i = 1; i + 1 < p1.size(); ++i) pass_through(site_index(p1[i]), p1[i - 1], p1[i + 1], k1);
