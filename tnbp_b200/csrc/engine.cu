@@ -464,6 +464,20 @@ size_t wave_budget_bytes() {
   }();
   return v;
 }
+// Largest sweep scratch one plan holds (TNBP_SCRATCH_CAP_MB, default 8
+// GiB): a sweep whose slots exceed it (a 10x10 lattice at D = 64 holds about
+// 140 GB of slots in one wave) runs in waves of this many bytes, so that the
+// slots fit beside the site tensors; a wave of 8 GiB still holds tens of
+// site tensors at D = 64, enough work for every SM.
+size_t scratch_cap_bytes() {
+  static const size_t v = [] {
+    const char* e = std::getenv("TNBP_SCRATCH_CAP_MB");
+    if (e && *e && std::strtoull(e, nullptr, 10) > 0) return (size_t)std::strtoull(e, nullptr, 10) << 20;
+    return size_t(8) << 30;
+  }();
+  return v;
+}
+
 static bool wave_budget_fixed() {
   const char* e = std::getenv("TNBP_WAVE_MB");
   return e && *e;
@@ -643,7 +657,7 @@ void Job::build_plan() {
   }
   // 2. waves of consecutive units within the byte budget (at least one unit)
   if (!tuning) choose_wave_budget();
-  const size_t budget = wave_budget;
+  const size_t budget = wave_budget && wave_budget < scratch_cap_bytes() ? wave_budget : scratch_cap_bytes();
   std::vector<std::vector<int>> waves;
   {
     size_t bytes = 0;
@@ -735,10 +749,9 @@ void Job::build_plan() {
         g1.Q = L * M;
         // chunks of about Q/16 rows (multiples of 64, 256..4096): FP64
         // partials of one sweep stay a small fraction of its traffic, and
-        // one wave of all sites gives every SM work; L2-sized waves of one
-        // unit use Q/128 so that each of their Gram launches fills the GPU
-        const long long div = budget ? 128 : 16;
-        long long cr = ((g1.Q / div) + 63) / 64 * 64;
+        // one wave of all sites gives every SM work.  The chunking does not
+        // depend on the wave budget, so neither does the rounding.
+        long long cr = ((g1.Q / 16) + 63) / 64 * 64;
         cr = std::max<long long>(256, std::min<long long>(4096, cr));
         g1.chunk_rows = cr;
         g1.nchunk = (int)((g1.Q + cr - 1) / cr);
@@ -1339,66 +1352,83 @@ struct ChainEntry {
   std::vector<int> dout;            // output dims
 };
 
+// Chain buffer capacity: chains run in batches whose intermediates fit in
+// this many bytes per buffer, so that truncating a large lattice (2 x 35 GB
+// of intermediates for a 10x10 lattice at D = 64 in complex128) needs two
+// bounded buffers instead.
+size_t chain_cap_bytes() { return size_t(8) << 30; }
+
 void Job::run_chains(std::vector<ChainEntry>& chains) {
   TNBP_TRACE_SCOPE("chains");
   if (chains.empty()) return;
-  size_t maxlen = 0;
-  std::vector<size_t> base(chains.size());
-  size_t tot = 0;
+  // largest intermediate of each chain (its input and final output live
+  // outside the chain buffers)
+  std::vector<size_t> inter(chains.size(), 0);
   for (size_t i = 0; i < chains.size(); ++i) {
     auto sh = site_shape(chains[i].site);
-    size_t n = site_elems(chains[i].site), mx = n;
-    for (size_t k = 0; k < chains[i].legs.size(); ++k) {
+    size_t n = site_elems(chains[i].site);
+    for (size_t k = 0; k + 1 < chains[i].legs.size(); ++k) {
       n = n / sh[chains[i].legs[k]] * chains[i].dout[k];
       sh[chains[i].legs[k]] = chains[i].dout[k];
-      mx = std::max(mx, n);
+      inter[i] = std::max(inter[i], n);
     }
-    base[i] = tot;
-    tot += align_elems(mx);
-    maxlen = std::max(maxlen, chains[i].legs.size());
   }
+  const size_t cap = chain_cap_bytes() / esz;
   DevBuf* buf = ws_chain;
-  buf[0].ensure(std::max<size_t>(tot, 32) * esz, stream);
-  buf[1].ensure(std::max<size_t>(tot, 32) * esz, stream);
-  for (size_t lv = 0; lv < maxlen; ++lv) {
-    std::vector<LegTask> t;
-    std::vector<long long> b;
-    long long nb = 0;
-    int maxdin = 1;
-    for (size_t i = 0; i < chains.size(); ++i) {
-      auto& c = chains[i];
-      if (lv >= c.legs.size()) continue;
-      auto sh = site_shape(c.site);
-      for (size_t k = 0; k < lv; ++k) sh[c.legs[k]] = c.dout[k];
-      const int leg = c.legs[lv];
-      long long L = 1, R = 1;
-      for (int k = 0; k < leg; ++k) L *= sh[k];
-      for (size_t k = leg + 1; k < sh.size(); ++k) R *= sh[k];
-      LegTask lt;
-      lt.in = lv == 0 ? c.src : static_cast<char*>(buf[(lv - 1) & 1].p) + base[i] * esz;
-      lt.out = (lv + 1 == c.legs.size()) ? c.dst : static_cast<char*>(buf[lv & 1].p) + base[i] * esz;
-      lt.mat = c.mats[lv];
-      lt.L = L; lt.R = R; lt.Din = sh[leg]; lt.Dout = c.dout[lv];
-      lt.block_begin = nb;
-      b.push_back(nb);
-      nb += (L * R + kRowTile - 1) / kRowTile;
-      maxdin = std::max(maxdin, lt.Din);
-      t.push_back(lt);
+  for (size_t i0 = 0; i0 < chains.size();) {
+    // the next batch: chains [i0, i1) whose intermediates fit one buffer
+    // (a single chain larger than the cap runs alone)
+    std::vector<size_t> base;
+    size_t tot = 0, i1 = i0, maxlen = 0;
+    while (i1 < chains.size() && (i1 == i0 || tot + align_elems(inter[i1]) <= cap)) {
+      base.push_back(tot);
+      tot += align_elems(inter[i1]);
+      maxlen = std::max(maxlen, chains[i1].legs.size());
+      ++i1;
     }
-    DevBuf dt, db;
-    upload_vec(dt, t, stream);
-    upload_vec(db, b, stream);
-    if (maxdin > 128) throw Error(TNBP_EUNSUPPORTED, "bond dimension above 128");
-    prepare_kernels(sprec);
-    if (sprec == TNBP_C128) {
-      const size_t smem = leg_smem<double>(maxdin);
-      (k_leg_apply<double><<<(unsigned)nb, kThreads, smem, stream>>>(static_cast<LegTask*>(dt.p), static_cast<long long*>(db.p), (int)t.size(), maxdin), note_launch());
-    } else {
-      const size_t smem = leg_smem<float>(maxdin);
-      (k_leg_apply<float><<<(unsigned)nb, kThreads, smem, stream>>>(static_cast<LegTask*>(dt.p), static_cast<long long*>(db.p), (int)t.size(), maxdin), note_launch());
+    buf[0].ensure(std::max<size_t>(tot, 32) * esz, stream);
+    buf[1].ensure(std::max<size_t>(tot, 32) * esz, stream);
+    for (size_t lv = 0; lv < maxlen; ++lv) {
+      std::vector<LegTask> t;
+      std::vector<long long> b;
+      long long nb = 0;
+      int maxdin = 1;
+      for (size_t i = i0; i < i1; ++i) {
+        auto& c = chains[i];
+        if (lv >= c.legs.size()) continue;
+        auto sh = site_shape(c.site);
+        for (size_t k = 0; k < lv; ++k) sh[c.legs[k]] = c.dout[k];
+        const int leg = c.legs[lv];
+        long long L = 1, R = 1;
+        for (int k = 0; k < leg; ++k) L *= sh[k];
+        for (size_t k = leg + 1; k < sh.size(); ++k) R *= sh[k];
+        LegTask lt;
+        lt.in = lv == 0 ? c.src : static_cast<char*>(buf[(lv - 1) & 1].p) + base[i - i0] * esz;
+        lt.out = (lv + 1 == c.legs.size()) ? c.dst : static_cast<char*>(buf[lv & 1].p) + base[i - i0] * esz;
+        lt.mat = c.mats[lv];
+        lt.L = L; lt.R = R; lt.Din = sh[leg]; lt.Dout = c.dout[lv];
+        lt.block_begin = nb;
+        b.push_back(nb);
+        nb += (L * R + kRowTile - 1) / kRowTile;
+        maxdin = std::max(maxdin, lt.Din);
+        t.push_back(lt);
+      }
+      DevBuf dt, db;
+      upload_vec(dt, t, stream);
+      upload_vec(db, b, stream);
+      if (maxdin > 128) throw Error(TNBP_EUNSUPPORTED, "bond dimension above 128");
+      prepare_kernels(sprec);
+      if (sprec == TNBP_C128) {
+        const size_t smem = leg_smem<double>(maxdin);
+        (k_leg_apply<double><<<(unsigned)nb, kThreads, smem, stream>>>(static_cast<LegTask*>(dt.p), static_cast<long long*>(db.p), (int)t.size(), maxdin), note_launch());
+      } else {
+        const size_t smem = leg_smem<float>(maxdin);
+        (k_leg_apply<float><<<(unsigned)nb, kThreads, smem, stream>>>(static_cast<LegTask*>(dt.p), static_cast<long long*>(db.p), (int)t.size(), maxdin), note_launch());
+      }
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(stream));
     }
-    CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(stream));
+    i0 = i1;
   }
 }
 

@@ -142,6 +142,8 @@ bool stop_on_growth(int prec, double prev, double c);
 inline bool reduced_sweeps(int prec) { return prec != TNBP_C128; }
 void prepare_kernels(int prec);
 size_t wave_budget_bytes();
+size_t scratch_cap_bytes();
+size_t chain_cap_bytes();
 bool autotune_enabled();
 bool tcgen05_enabled();
 bool bulk_leg_enabled();

@@ -67,10 +67,10 @@ static int sweep_slots(int g) {
 
 // Peak device bytes of a job on `edges` whose BP runs at bond dimension
 // D[e] on edge e (physical dimension 2): per site the tensor, its spare
-// buffer, the two chain buffers of truncation and the complex64 sweep copy
-// (TNBP_MIXED); the sweep scratch slots of the largest wave; both message arenas
-// twice; per-edge truncation work and Gram partials; plus extra_bytes; 10 %
-// and 8 MiB of margin.
+// buffer and the complex64 sweep copy (TNBP_MIXED); the two chain buffers of
+// truncation and measurement (at most the chain cap each); the sweep scratch
+// slots of the largest wave; both message arenas twice; per-edge truncation
+// work and Gram partials; plus extra_bytes; 10 % and 8 MiB of margin.
 uint64_t footprint_estimate(const std::vector<std::pair<int, int>>& edges, const std::vector<double>& D, int prec,
                             uint64_t extra_bytes) {
   const double esz = prec == TNBP_C64 ? 8.0 : 16.0;   // stored element
@@ -87,16 +87,20 @@ uint64_t footprint_estimate(const std::vector<std::pair<int, int>>& edges, const
       n[pos[v]] *= D[e];
       ++deg[pos[v]];
     }
-  double bytes = 0.0, slots_all = 0.0, unit_max = 0.0;
+  double bytes = 0.0, slots_all = 0.0, unit_max = 0.0, chain_all = 0.0;
   for (size_t i = 0; i < sites.size(); ++i) {
-    bytes += n[i] * (4.0 * esz + shadow);  // V, spare, 2 chain buffers, sweep copy
+    bytes += n[i] * (2.0 * esz + shadow);  // V, spare, sweep copy
+    chain_all += n[i] * esz;
     slots_all += n[i] * wsz * sweep_slots(deg[i]);
     unit_max = std::max(unit_max, n[i] * wsz * std::max(1, deg[i]));
   }
+  bytes += 2.0 * std::min(chain_all, (double)chain_cap_bytes());
   // sweep scratch: one wave's units at a time (a wave stays within the wave
-  // budget unless it is a single unit), all of them without a budget
-  const double wave = (double)wave_budget_bytes();
-  bytes += wave > 0.0 ? std::min(slots_all, std::max(wave, unit_max)) : slots_all;
+  // budget, at most the scratch cap, unless it is a single unit)
+  const double cap = (double)scratch_cap_bytes();
+  double wave = (double)wave_budget_bytes();
+  if (wave <= 0.0 || wave > cap) wave = cap;
+  bytes += std::min(slots_all, std::max(wave, unit_max));
   for (size_t e = 0; e < ne; ++e) {
     const double dd = D[e] * D[e];
     bytes += 4.0 * 2.0 * dd * esz;   // message arenas (old + new)
