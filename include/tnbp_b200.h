@@ -410,6 +410,23 @@ int tnbp_server_step(tnbp_server* srv, int32_t* n_active_out, int32_t* n_queued_
    A CUDA error fails tnbp_server_step itself. */
 int tnbp_server_result(tnbp_server* srv, int64_t request_id, double* sum_out,
                        int32_t* pending_out);
+/* Precision escalation (no counterpart in tnbp, whose estimator runs one
+   precision): with on != 0, a TNBP_C64 or TNBP_MIXED server restarts, from
+   |0...0> and in complex128, every request whose BP loop ends at its
+   iteration limit without reaching its tolerance (the BeliefPropagation loop
+   of apps/estimator/main.cc:131-157 running out of sweeps).  Non-converging
+   BP is ill-conditioned: the messages after the last sweep carry every
+   rounding of the earlier steps, amplified, so only the complex128 run
+   reproduces the plain path's value.  Off by default; no effect on a
+   TNBP_C128 server.  Requests already admitted keep running. */
+int tnbp_server_set_escalation(tnbp_server* srv, int32_t on);
+/* How a request ran: *precision_out = the precision of its last run,
+   *escalated_out = 1 if it was restarted in complex128,
+   *bp_converged_out = 1 if every BP loop of its last run reached its
+   tolerance (0 if some loop stopped at the iteration limit).  Any pointer
+   may be NULL; valid for queued, running and finished requests. */
+int tnbp_server_request_info(tnbp_server* srv, int64_t request_id, int32_t* precision_out,
+                             int32_t* escalated_out, int32_t* bp_converged_out);
 
 #ifdef __cplusplus
 }

@@ -475,6 +475,17 @@ class Server {
     return true;
   }
   void cancel(int64_t id) { check(tnbp_server_cancel(srv_, id)); }
+  /* Restart non-converging requests in complex128 (reduced-precision servers). */
+  void set_escalation(bool on) { check(tnbp_server_set_escalation(srv_, on ? 1 : 0)); }
+  struct RequestInfo {
+    int precision;
+    bool escalated, bp_converged;
+  };
+  RequestInfo info(int64_t id) {
+    int32_t p = 0, e = 0, c = 0;
+    check(tnbp_server_request_info(srv_, id, &p, &e, &c));
+    return RequestInfo{p, e != 0, c != 0};
+  }
 
  private:
   tnbp_server* srv_ = nullptr;

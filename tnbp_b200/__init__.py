@@ -100,6 +100,8 @@ _SIGS = {
     "tnbp_server_cancel": [_vp, C.c_int64],
     "tnbp_server_step": [_vp, _i32p, _i32p, _i32p],
     "tnbp_server_result": [_vp, C.c_int64, _f64p, _i32p],
+    "tnbp_server_set_escalation": [_vp, C.c_int32],
+    "tnbp_server_request_info": [_vp, C.c_int64, _i32p, _i32p, _i32p],
 }
 for _n, _a in _SIGS.items():
     _f = getattr(lib, _n)
@@ -664,6 +666,18 @@ class Server:
         a, q, d = C.c_int32(), C.c_int32(), C.c_int32()
         _chk(lib.tnbp_server_step(self.h, C.byref(a), C.byref(q), C.byref(d)))
         return a.value, q.value, d.value
+
+    def set_escalation(self, on=True):
+        """Restart, in complex128, requests whose BP loop does not converge
+        (tnbp_server_set_escalation; reduced-precision servers only)."""
+        _chk(lib.tnbp_server_set_escalation(self.h, 1 if on else 0))
+
+    def info(self, rid):
+        """{'precision', 'escalated', 'bp_converged'} of a request
+        (tnbp_server_request_info)."""
+        p, e, c = C.c_int32(), C.c_int32(), C.c_int32()
+        _chk(lib.tnbp_server_request_info(self.h, rid, C.byref(p), C.byref(e), C.byref(c)))
+        return {"precision": p.value, "escalated": bool(e.value), "bp_converged": bool(c.value)}
 
     def result(self, rid):
         out = np.zeros(2, np.float64)

@@ -127,7 +127,7 @@ uint64_t Server::footprint(const Request& r) const {
       prod *= ts.layers[r.source == Request::QASM ? t : 0]->rank[e];
     D[e] = std::max(1.0, std::min(cap, prod));
   }
-  return footprint_estimate(edges, D, prec, ts.device_bytes);
+  return footprint_estimate(edges, D, r.prec, ts.device_bytes);
 }
 
 // The TPO layers of a circuit, built and uploaded on the first request that
@@ -176,6 +176,7 @@ int64_t Server::submit(std::unique_ptr<Request> r) {
   if (!r->tpos) throw Error(TNBP_EINVAL, "request without TPO layers");
   if (r->source == Request::KICKED_ISING && r->L < 2) throw Error(TNBP_EINVAL, "lattice side must be >= 2");
   if (r->chi < 1 || r->steps < 0 || r->maxit < 0) throw Error(TNBP_EINVAL, "bad request parameters");
+  r->prec = prec;
   r->footprint = footprint(*r);
   if (r->footprint > budget) throw Error(TNBP_ENOMEM, "request footprint exceeds the server's HBM budget");
   r->id = next_id++;
@@ -189,8 +190,9 @@ void Server::start(Request& r) {
   const auto& edges = r.tpos->edges;
   std::vector<int32_t> e(2 * edges.size());
   for (size_t i = 0; i < edges.size(); ++i) { e[2 * i] = edges[i].first; e[2 * i + 1] = edges[i].second; }
-  r.job = std::make_unique<Job>(e.data(), (int64_t)edges.size(), nullptr, prec, stream, 0);
+  r.job = std::make_unique<Job>(e.data(), (int64_t)edges.size(), nullptr, r.prec, stream, 0);
   r.step = 0;
+  r.bp_converged = true;
   r.phase = r.steps > 0 ? Request::ABSORB : Request::MEASURE;
 }
 
@@ -255,6 +257,106 @@ void Server::cancel(int64_t id) {
   fail(r, TNBP_ECANCELED, "request cancelled");
 }
 
+// Restart a request from |0...0> in complex128 (see Server::escalate); its
+// footprint is re-counted for the complex128 job.
+void Server::restart_c128(Request& r) {
+  r.job.reset();
+  in_use -= r.footprint;
+  r.prec = TNBP_C128;
+  r.escalated = true;
+  r.footprint = footprint(r);
+  in_use += r.footprint;
+  start(r);
+}
+
+// One batched BP sweep over the requests of `grp`, whose jobs all have
+// precision gprec, and the BP-loop decision of each request.
+void Server::sweep_group(int gprec, const std::vector<Request*>& inbp) {
+  TNBP_TRACE_SCOPE("server.3_sweep");
+  std::vector<BatchEntry> entries;
+  for (auto* r : inbp) {
+    r->job->sync_shadow();
+    if (!r->job->plan.valid) r->job->build_plan();
+    entries.push_back({r->job.get(), r->job->cur});
+  }
+  prepare_kernels(gprec);
+  std::vector<uint64_t> key;
+  for (auto& e : entries) key.push_back(2 * e.job->plan_serial + (uint64_t)e.parity);
+  auto it = sweeps.find(key);
+  if (it == sweeps.end()) {
+    auto cs = std::make_unique<CachedSweep>();
+    build_batch(entries, cs->batch, stream);
+    it = sweeps.emplace(key, std::move(cs)).first;
+    sweeps_lru.push_back(key);
+    while (sweeps.size() > sweeps_cap) {
+      sweeps.erase(sweeps_lru.front());
+      sweeps_lru.pop_front();
+    }
+  } else {
+    sweeps_lru.remove(key);
+    sweeps_lru.push_back(key);
+  }
+  CachedSweep& cs = *it->second;
+  SweepBatch& batch = cs.batch;
+  if (cs.uses == 1 && !batch.graph) {
+    TNBP_TRACE_SCOPE("server.3_graph_capture");
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      batch.nkernels = launch_batch(batch, gprec, stream);
+    } catch (...) {
+      cudaStreamEndCapture(stream, &graph);
+      throw;
+    }
+    CK(cudaStreamEndCapture(stream, &graph));
+    CK(cudaGraphInstantiate(&batch.graph, graph, 0));
+    cudaGraphDestroy(graph);
+  }
+  if (batch.graph) {
+    CK(cudaGraphLaunch(batch.graph, stream));
+    note_launch(batch.nkernels);
+    ++graph_launches;
+  } else {
+    note_launch(launch_batch(batch, gprec, stream));
+    ++eager_launches;
+  }
+  ++cs.uses;
+  if (hcond_cap < entries.size()) {
+    if (hcond) cudaFreeHost(hcond);
+    hcond_cap = std::max<size_t>(64, 2 * entries.size());
+    CK(cudaMallocHost(&hcond, hcond_cap * sizeof(double)));
+  }
+  CK(cudaMemcpyAsync(hcond, batch.cond.p, entries.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  if (reduced_sweeps(gprec)) check_tc_error(stream);
+  for (size_t i = 0; i < inbp.size(); ++i) {
+    Request& r = *inbp[i];
+    Job& j = *r.job;
+    if (r.bp_iters == 0) {  // first sweep of the loop: always kept
+      j.cur = 1 - j.cur;
+      r.bp_iters = 1;
+      continue;
+    }
+    const double c = hcond[i];
+    if (!std::isfinite(c)) {
+      fail(r, TNBP_ENOTCONV, "BP condition is not finite (non-finite messages)");
+      continue;
+    }
+    const bool conv = c < effective_tol(gprec, r.tol);
+    if (conv || r.bp_iters >= r.maxit || stop_on_growth(gprec, r.prev_cond, c)) {
+      r.phase = Request::TRUNC;  // keep the current messages
+      if (!conv && r.bp_iters >= r.maxit) {
+        r.bp_converged = false;
+        if (escalate && r.prec != TNBP_C128) restart_c128(r);
+      }
+    } else {
+      r.prev_cond = c;
+      j.cur = 1 - j.cur;
+      ++r.bp_iters;
+    }
+  }
+}
+
 void Server::step(int* n_active, int* n_queued, int* n_done) {
   TNBP_TRACE_SCOPE("server.step");
   int done = 0;
@@ -279,93 +381,16 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
       if (r.maxit <= 0) r.phase = Request::TRUNC;
     }
   }
-  // 3. one batched BP sweep over every request in its BP phase
-  std::vector<BatchEntry> entries;
-  std::vector<Request*> inbp;
-  for (int64_t id : active) {
-    Request& r = *reqs[id];
-    if (r.phase == Request::BP) {
-      entries.push_back({r.job.get(), r.job->cur});
-      inbp.push_back(&r);
+  // 3. one batched BP sweep over every request in its BP phase, one batch
+  // per job precision (requests escalated to complex128 sweep apart)
+  {
+    std::vector<Request*> grp[2];
+    for (int64_t id : active) {
+      Request& r = *reqs[id];
+      if (r.phase == Request::BP) grp[r.prec == prec ? 0 : 1].push_back(&r);
     }
-  }
-  if (!entries.empty()) {
-    TNBP_TRACE_SCOPE("server.3_sweep");
-    for (auto* r : inbp) {
-      r->job->sync_shadow();
-      if (!r->job->plan.valid) r->job->build_plan();
-    }
-    prepare_kernels(prec);
-    std::vector<uint64_t> key;
-    for (auto& e : entries) key.push_back(2 * e.job->plan_serial + (uint64_t)e.parity);
-    auto it = sweeps.find(key);
-    if (it == sweeps.end()) {
-      auto cs = std::make_unique<CachedSweep>();
-      build_batch(entries, cs->batch, stream);
-      it = sweeps.emplace(key, std::move(cs)).first;
-      sweeps_lru.push_back(key);
-      while (sweeps.size() > sweeps_cap) {
-        sweeps.erase(sweeps_lru.front());
-        sweeps_lru.pop_front();
-      }
-    } else {
-      sweeps_lru.remove(key);
-      sweeps_lru.push_back(key);
-    }
-    CachedSweep& cs = *it->second;
-    SweepBatch& batch = cs.batch;
-    if (cs.uses == 1 && !batch.graph) {
-      TNBP_TRACE_SCOPE("server.3_graph_capture");
-      cudaGraph_t graph;
-      CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-      try {
-        batch.nkernels = launch_batch(batch, prec, stream);
-      } catch (...) {
-        cudaStreamEndCapture(stream, &graph);
-        throw;
-      }
-      CK(cudaStreamEndCapture(stream, &graph));
-      CK(cudaGraphInstantiate(&batch.graph, graph, 0));
-      cudaGraphDestroy(graph);
-    }
-    if (batch.graph) {
-      CK(cudaGraphLaunch(batch.graph, stream));
-      note_launch(batch.nkernels);
-      ++graph_launches;
-    } else {
-      note_launch(launch_batch(batch, prec, stream));
-      ++eager_launches;
-    }
-    ++cs.uses;
-    if (hcond_cap < entries.size()) {
-      if (hcond) cudaFreeHost(hcond);
-      hcond_cap = std::max<size_t>(64, 2 * entries.size());
-      CK(cudaMallocHost(&hcond, hcond_cap * sizeof(double)));
-    }
-    CK(cudaMemcpyAsync(hcond, batch.cond.p, entries.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
-    CK(cudaStreamSynchronize(stream));
-    if (reduced_sweeps(prec)) check_tc_error(stream);
-    for (size_t i = 0; i < inbp.size(); ++i) {
-      Request& r = *inbp[i];
-      Job& j = *r.job;
-      if (r.bp_iters == 0) {  // first sweep of the loop: always kept
-        j.cur = 1 - j.cur;
-        r.bp_iters = 1;
-        continue;
-      }
-      const double c = hcond[i];
-      if (!std::isfinite(c)) {
-        fail(r, TNBP_ENOTCONV, "BP condition is not finite (non-finite messages)");
-        continue;
-      }
-      if (c < effective_tol(prec, r.tol) || r.bp_iters >= r.maxit || stop_on_growth(prec, r.prev_cond, c)) {
-        r.phase = Request::TRUNC;  // keep the current messages
-      } else {
-        r.prev_cond = c;
-        j.cur = 1 - j.cur;
-        ++r.bp_iters;
-      }
-    }
+    if (!grp[0].empty()) sweep_group(prec, grp[0]);
+    if (!grp[1].empty()) sweep_group(TNBP_C128, grp[1]);
   }
   // 4. truncation, next step or measurement
   TNBP_TRACE_SCOPE("server.4_trunc_measure");
@@ -563,6 +588,26 @@ int tnbp_server_result(tnbp_server* srv, int64_t id, double* sum, int32_t* pendi
     if (pending) *pending = done ? 0 : 1;
     if (done && it->second->error_code) throw tnbp::Error(it->second->error_code, it->second->error);
     if (sum && done) { sum[0] = it->second->result[0]; sum[1] = it->second->result[1]; }
+  });
+}
+
+int tnbp_server_set_escalation(tnbp_server* srv, int32_t on) {
+  return sguard([&] {
+    if (!srv) throw tnbp::Error(TNBP_EINVAL, "server is NULL");
+    srv->s->escalate = on != 0;
+  });
+}
+
+int tnbp_server_request_info(tnbp_server* srv, int64_t id, int32_t* precision, int32_t* escalated,
+                             int32_t* bp_converged) {
+  return sguard([&] {
+    if (!srv) throw tnbp::Error(TNBP_EINVAL, "server is NULL");
+    auto it = srv->s->reqs.find(id);
+    if (it == srv->s->reqs.end()) throw tnbp::Error(TNBP_EINVAL, "unknown request id");
+    const tnbp::Request& r = *it->second;
+    if (precision) *precision = r.prec;
+    if (escalated) *escalated = r.escalated ? 1 : 0;
+    if (bp_converged) *bp_converged = r.bp_converged ? 1 : 0;
   });
 }
 

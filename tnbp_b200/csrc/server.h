@@ -46,6 +46,9 @@ struct Request {
   int step = 0, bp_iters = 0;
   double prev_cond = 0;
   uint64_t footprint = 0;
+  int prec = 0;               // precision of the request's job (the server's, or TNBP_C128 once escalated)
+  bool escalated = false;     // restarted in complex128 after a BP loop that did not converge
+  bool bp_converged = true;   // every BP loop of the (last) run reached its tolerance
   double result[2] = {0, 0};
   int error_code = 0;  // a request that failed keeps its error; others go on
   std::string error;
@@ -54,6 +57,12 @@ struct Request {
 struct Server {
   int prec;
   uint64_t budget;
+  // Reduced-precision server (TNBP_C64 / TNBP_MIXED): a request whose BP loop
+  // ends at its iteration limit without reaching its tolerance is restarted
+  // from |0...0> in complex128.  Where BP does not converge, the messages
+  // after the iteration limit depend on every rounding of the earlier steps,
+  // so only the complex128 run reproduces the plain path's value.
+  bool escalate = false;
   int max_active;
   cudaStream_t stream = nullptr;
   double* hcond = nullptr;
@@ -90,6 +99,8 @@ struct Server {
                                         const std::function<void(tnbp_host::Edges&,
                                                                  std::vector<tnbp_host::Layer>&)>& build);
   void step(int* n_active, int* n_queued, int* n_done);
+  void sweep_group(int gprec, const std::vector<Request*>& grp);
+  void restart_c128(Request& r);
   uint64_t footprint(const Request& r) const;
   void start(Request& r);
   void finish(Request& r);
