@@ -327,7 +327,7 @@ def served_summary(tb, n):
     esc, lat_e, span_e, info_e, rejected = run_served(tb, reqs, tb.MIXED, escalate=True)
     mix, lat_m, span_m, _, _ = run_served(tb, reqs, tb.MIXED, escalate=False)
     plain, lat_p, span_p, conv = run_plain_fifo(tb, reqs, tb.C128, skip=set(rejected))
-    kept = sorted(plain)
+    kept = sorted(set(plain) & set(esc) & set(mix))
     dE_e = [abs(esc[i] - plain[i]) for i in kept]
     dE_m = [abs(mix[i] - plain[i]) for i in kept]
 

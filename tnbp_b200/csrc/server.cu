@@ -42,8 +42,18 @@ Server::Server(int precision, uint64_t budget_bytes, int max_active_jobs)
   keep_pool_memory();
   CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   if (budget == 0) {
+    // free device memory plus what the stream-ordered pool holds unused
+    // (the engine keeps freed blocks in the pool, see keep_pool_memory)
     size_t fr = 0, tot = 0;
     CK(cudaMemGetInfo(&fr, &tot));
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t reserved = 0, used = 0;
+    CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+    if (reserved > used) fr += (size_t)(reserved - used);
     const size_t reserve = (size_t)4 << 30;
     budget = fr > 2 * reserve ? fr - reserve : fr / 2;
   }
