@@ -464,11 +464,14 @@ size_t wave_budget_bytes() {
   }();
   return v;
 }
-// Largest sweep scratch one plan holds (TNBP_SCRATCH_CAP_MB, default 8
-// GiB): a sweep whose slots exceed it (a 10x10 lattice at D = 64 holds about
-// 140 GB of slots in one wave) runs in waves of this many bytes, so that the
-// slots fit beside the site tensors; a wave of 8 GiB still holds tens of
-// site tensors at D = 64, enough work for every SM.
+// Sweep scratch a served job's plan holds at most (TNBP_SCRATCH_CAP_MB,
+// default 8 GiB; the server's footprint estimate counts the same): a sweep
+// whose slots exceed it (a 10x10 lattice at D = 64 holds about 140 GB of
+// slots in one wave) runs in waves of this many bytes; a wave of 8 GiB still
+// holds tens of site tensors at D = 64, enough work for every SM.  A job
+// created on its own (tnbp_job_create) keeps one wave while its slots fit in
+// half of the device memory still available (Job::scratch_limit): on the
+// 16x16 D = 32 workload three 8 GiB waves made the solve 30 % slower than one.
 size_t scratch_cap_bytes() {
   static const size_t v = [] {
     const char* e = std::getenv("TNBP_SCRATCH_CAP_MB");
@@ -476,6 +479,27 @@ size_t scratch_cap_bytes() {
     return size_t(8) << 30;
   }();
   return v;
+}
+
+// Free device memory plus what the stream-ordered pool holds unused (the
+// engine keeps freed blocks in the pool, see keep_pool_memory).
+size_t device_bytes_available() {
+  size_t fr = 0, tot = 0;
+  CK(cudaMemGetInfo(&fr, &tot));
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  cudaMemPool_t pool;
+  CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+  uint64_t reserved = 0, used = 0;
+  CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+  CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+  if (reserved > used) fr += (size_t)(reserved - used);
+  return fr;
+}
+
+size_t Job::scratch_limit() const {
+  if (scratch_cap) return scratch_cap;
+  return std::max(scratch_cap_bytes(), (device_bytes_available() + ws_scratch.bytes) / 2);
 }
 
 static bool wave_budget_fixed() {
@@ -488,7 +512,8 @@ static bool wave_budget_fixed() {
 // first time a job of a class with a large sweep (at least 2e11 algorithmic
 // flops) starts a BP loop, each candidate budget gets a plan, one warm-up
 // sweep and two timed sweeps (CUDA events), all writing only the message
-// arena the loop overwrites next, and the fastest is kept.  The wave budget
+// arena the loop overwrites next, and the fastest is kept (a candidate must
+// beat the one before it by 3 %).  The wave budget
 // only groups tasks into launches; every task's kernel and arithmetic are the
 // same under every budget, so tuning never changes a result.  Choices are
 // kept in a table per device (name and SM count) in $TNBP_TUNE_DIR (default
@@ -503,7 +528,10 @@ bool autotune_enabled() {
 }
 
 namespace {
-constexpr size_t kWaveCandidatesMb[] = {32, 64, 96, 128, 192, 0};
+// one wave first: the largest scratch is allocated once and every later
+// candidate reuses it (the buffer only grows), so tuning does not churn the
+// allocator
+constexpr size_t kWaveCandidatesMb[] = {0, 32, 64, 96, 128, 192};
 constexpr double kTuneMinFlops = 2e11;
 
 struct TuneTable {
@@ -605,7 +633,9 @@ void Job::autotune_waves() {
     if (reduced_sweeps(prec)) check_tc_error(stream);
     ms /= 2.0;
     if (mb == (wave_budget_bytes() >> 20)) default_ms = ms;
-    if (ms < best_ms) { best_ms = ms; best_mb = mb; }
+    // a later (smaller) budget must be 3 % faster to replace an earlier one:
+    // two timed sweeps do not resolve smaller differences
+    if (ms < 0.97 * best_ms) { best_ms = ms; best_mb = mb; }
   }
   wave_budget = best_mb << 20;
   destroy_graphs();
@@ -657,7 +687,8 @@ void Job::build_plan() {
   }
   // 2. waves of consecutive units within the byte budget (at least one unit)
   if (!tuning) choose_wave_budget();
-  const size_t budget = wave_budget && wave_budget < scratch_cap_bytes() ? wave_budget : scratch_cap_bytes();
+  const size_t cap = scratch_limit();
+  const size_t budget = wave_budget && wave_budget < cap ? wave_budget : cap;
   std::vector<std::vector<int>> waves;
   {
     size_t bytes = 0;

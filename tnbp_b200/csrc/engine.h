@@ -143,6 +143,7 @@ inline bool reduced_sweeps(int prec) { return prec != TNBP_C128; }
 void prepare_kernels(int prec);
 size_t wave_budget_bytes();
 size_t scratch_cap_bytes();
+size_t device_bytes_available();
 size_t chain_cap_bytes();
 bool autotune_enabled();
 bool tcgen05_enabled();
@@ -219,6 +220,7 @@ struct Job {
   SweepPlan plan;
   uint64_t plan_serial = 0;  // unique per plan build (keys of the server's sweep graphs)
   size_t wave_budget = 0;    // wave byte budget of the next plan (0: one wave)
+  size_t scratch_cap = 0;    // most sweep-slot bytes a plan may hold (0: from free device memory)
   bool tuning = false;       // the autotuner sets wave_budget itself
   long long sweeps_run = 0;
   float last_sweep_ms = 0.f;
@@ -240,6 +242,7 @@ struct Job {
   void* mptr(int arena, int m) const;
   void destroy_graphs();
   void build_plan();
+  size_t scratch_limit() const;
   void run_sweep(int par);
   double read_cond();
   void bp_sweep();

@@ -42,18 +42,7 @@ Server::Server(int precision, uint64_t budget_bytes, int max_active_jobs)
   keep_pool_memory();
   CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   if (budget == 0) {
-    // free device memory plus what the stream-ordered pool holds unused
-    // (the engine keeps freed blocks in the pool, see keep_pool_memory)
-    size_t fr = 0, tot = 0;
-    CK(cudaMemGetInfo(&fr, &tot));
-    int dev = 0;
-    CK(cudaGetDevice(&dev));
-    cudaMemPool_t pool;
-    CK(cudaDeviceGetDefaultMemPool(&pool, dev));
-    uint64_t reserved = 0, used = 0;
-    CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
-    CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
-    if (reserved > used) fr += (size_t)(reserved - used);
+    const size_t fr = device_bytes_available();
     const size_t reserve = (size_t)4 << 30;
     budget = fr > 2 * reserve ? fr - reserve : fr / 2;
   }
@@ -201,6 +190,7 @@ void Server::start(Request& r) {
   std::vector<int32_t> e(2 * edges.size());
   for (size_t i = 0; i < edges.size(); ++i) { e[2 * i] = edges[i].first; e[2 * i + 1] = edges[i].second; }
   r.job = std::make_unique<Job>(e.data(), (int64_t)edges.size(), nullptr, r.prec, stream, 0);
+  r.job->scratch_cap = scratch_cap_bytes();  // the footprint estimate counts this cap
   r.step = 0;
   r.bp_converged = true;
   r.phase = r.steps > 0 ? Request::ABSORB : Request::MEASURE;
