@@ -427,6 +427,23 @@ int tnbp_server_set_escalation(tnbp_server* srv, int32_t on);
    may be NULL; valid for queued, running and finished requests. */
 int tnbp_server_request_info(tnbp_server* srv, int64_t request_id, int32_t* precision_out,
                              int32_t* escalated_out, int32_t* bp_converged_out);
+/* Escalation threshold (no counterpart in tnbp): with escalation on, a
+   request is restarted in complex128 only when the BP loop that ran out of
+   sweeps never brought its condition (the mean message change per sweep,
+   bp.h:266-355) below min_cond.  0 (the default) escalates on every loop
+   that runs out of sweeps.  A loop whose condition came down to a small value
+   and hovers there (a slow approach, a small limit cycle, the reduced
+   precision's rounding floor) leaves messages that rounding moves little; a
+   loop whose condition stays of order one is the ill-conditioned case.
+   min_cond must be finite and >= 0 (TNBP_EINVAL otherwise). */
+int tnbp_server_set_escalation_threshold(tnbp_server* srv, double min_cond);
+/* BP statistics of a request's last run: *unconverged_loops_out = BP loops
+   that stopped at the iteration limit, *worst_final_cond_out = the largest
+   final condition among them, *worst_min_cond_out = the largest of their
+   smallest conditions (0 when every loop converged).  Any pointer may be
+   NULL. */
+int tnbp_server_request_bp_stats(tnbp_server* srv, int64_t request_id, int32_t* unconverged_loops_out,
+                                 double* worst_final_cond_out, double* worst_min_cond_out);
 
 #ifdef __cplusplus
 }

@@ -477,14 +477,20 @@ class Server {
   void cancel(int64_t id) { check(tnbp_server_cancel(srv_, id)); }
   /* Restart non-converging requests in complex128 (reduced-precision servers). */
   void set_escalation(bool on) { check(tnbp_server_set_escalation(srv_, on ? 1 : 0)); }
+  /* Escalate only loops whose condition never fell below min_cond. */
+  void set_escalation_threshold(double min_cond) { check(tnbp_server_set_escalation_threshold(srv_, min_cond)); }
   struct RequestInfo {
     int precision;
     bool escalated, bp_converged;
+    int unconverged_loops;
+    double worst_final_cond, worst_min_cond;
   };
   RequestInfo info(int64_t id) {
-    int32_t p = 0, e = 0, c = 0;
+    int32_t p = 0, e = 0, c = 0, n = 0;
+    double wf = 0.0, wm = 0.0;
     check(tnbp_server_request_info(srv_, id, &p, &e, &c));
-    return RequestInfo{p, e != 0, c != 0};
+    check(tnbp_server_request_bp_stats(srv_, id, &n, &wf, &wm));
+    return RequestInfo{p, e != 0, c != 0, n, wf, wm};
   }
 
  private:

@@ -102,6 +102,8 @@ _SIGS = {
     "tnbp_server_result": [_vp, C.c_int64, _f64p, _i32p],
     "tnbp_server_set_escalation": [_vp, C.c_int32],
     "tnbp_server_request_info": [_vp, C.c_int64, _i32p, _i32p, _i32p],
+    "tnbp_server_set_escalation_threshold": [_vp, C.c_double],
+    "tnbp_server_request_bp_stats": [_vp, C.c_int64, _i32p, _f64p, _f64p],
 }
 for _n, _a in _SIGS.items():
     _f = getattr(lib, _n)
@@ -672,12 +674,21 @@ class Server:
         (tnbp_server_set_escalation; reduced-precision servers only)."""
         _chk(lib.tnbp_server_set_escalation(self.h, 1 if on else 0))
 
+    def set_escalation_threshold(self, min_cond):
+        """Escalate only loops whose condition never fell below min_cond
+        (tnbp_server_set_escalation_threshold; 0 = every non-converging loop)."""
+        _chk(lib.tnbp_server_set_escalation_threshold(self.h, float(min_cond)))
+
     def info(self, rid):
-        """{'precision', 'escalated', 'bp_converged'} of a request
-        (tnbp_server_request_info)."""
+        """{'precision', 'escalated', 'bp_converged', 'unconverged_loops',
+        'worst_final_cond', 'worst_min_cond'} of a request
+        (tnbp_server_request_info, tnbp_server_request_bp_stats)."""
         p, e, c = C.c_int32(), C.c_int32(), C.c_int32()
         _chk(lib.tnbp_server_request_info(self.h, rid, C.byref(p), C.byref(e), C.byref(c)))
-        return {"precision": p.value, "escalated": bool(e.value), "bp_converged": bool(c.value)}
+        n, wf, wm = C.c_int32(), C.c_double(), C.c_double()
+        _chk(lib.tnbp_server_request_bp_stats(self.h, rid, C.byref(n), C.byref(wf), C.byref(wm)))
+        return {"precision": p.value, "escalated": bool(e.value), "bp_converged": bool(c.value),
+                "unconverged_loops": n.value, "worst_final_cond": wf.value, "worst_min_cond": wm.value}
 
     def result(self, rid):
         out = np.zeros(2, np.float64)

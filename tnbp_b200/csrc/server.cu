@@ -193,6 +193,9 @@ void Server::start(Request& r) {
   r.job->scratch_cap = scratch_cap_bytes();  // the footprint estimate counts this cap
   r.step = 0;
   r.bp_converged = true;
+  r.unconv_loops = 0;
+  r.worst_final_cond = 0;
+  r.worst_min_cond = 0;
   r.phase = r.steps > 0 ? Request::ABSORB : Request::MEASURE;
 }
 
@@ -343,11 +346,15 @@ void Server::sweep_group(int gprec, const std::vector<Request*>& inbp) {
       continue;
     }
     const bool conv = c < effective_tol(gprec, r.tol);
+    r.loop_min_cond = std::min(r.loop_min_cond, c);
     if (conv || r.bp_iters >= r.maxit || stop_on_growth(gprec, r.prev_cond, c)) {
       r.phase = Request::TRUNC;  // keep the current messages
       if (!conv && r.bp_iters >= r.maxit) {
         r.bp_converged = false;
-        if (escalate && r.prec != TNBP_C128) restart_c128(r);
+        ++r.unconv_loops;
+        r.worst_final_cond = std::max(r.worst_final_cond, c);
+        r.worst_min_cond = std::max(r.worst_min_cond, r.loop_min_cond);
+        if (escalate && r.prec != TNBP_C128 && r.loop_min_cond > escalate_min_cond) restart_c128(r);
       }
     } else {
       r.prev_cond = c;
@@ -378,6 +385,7 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
       r.phase = Request::BP;
       r.bp_iters = 0;
       r.prev_cond = INFINITY;
+      r.loop_min_cond = INFINITY;
       if (r.maxit <= 0) r.phase = Request::TRUNC;
     }
   }
@@ -595,6 +603,28 @@ int tnbp_server_set_escalation(tnbp_server* srv, int32_t on) {
   return sguard([&] {
     if (!srv) throw tnbp::Error(TNBP_EINVAL, "server is NULL");
     srv->s->escalate = on != 0;
+  });
+}
+
+int tnbp_server_set_escalation_threshold(tnbp_server* srv, double min_cond) {
+  return sguard([&] {
+    if (!srv) throw tnbp::Error(TNBP_EINVAL, "server is NULL");
+    if (!(min_cond >= 0.0) || !std::isfinite(min_cond))
+      throw tnbp::Error(TNBP_EINVAL, "escalation threshold must be finite and >= 0");
+    srv->s->escalate_min_cond = min_cond;
+  });
+}
+
+int tnbp_server_request_bp_stats(tnbp_server* srv, int64_t id, int32_t* unconverged_loops,
+                                 double* worst_final_cond, double* worst_min_cond) {
+  return sguard([&] {
+    if (!srv) throw tnbp::Error(TNBP_EINVAL, "server is NULL");
+    auto it = srv->s->reqs.find(id);
+    if (it == srv->s->reqs.end()) throw tnbp::Error(TNBP_EINVAL, "unknown request id");
+    const tnbp::Request& r = *it->second;
+    if (unconverged_loops) *unconverged_loops = r.unconv_loops;
+    if (worst_final_cond) *worst_final_cond = r.worst_final_cond;
+    if (worst_min_cond) *worst_min_cond = r.worst_min_cond;
   });
 }
 

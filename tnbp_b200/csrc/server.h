@@ -49,6 +49,12 @@ struct Request {
   int prec = 0;               // precision of the request's job (the server's, or TNBP_C128 once escalated)
   bool escalated = false;     // restarted in complex128 after a BP loop that did not converge
   bool bp_converged = true;   // every BP loop of the (last) run reached its tolerance
+  // BP loops of the (last) run that stopped at the iteration limit, the
+  // largest final condition among them and the largest of their smallest
+  // conditions (how close the closest of them came to converging)
+  int unconv_loops = 0;
+  double worst_final_cond = 0, worst_min_cond = 0;
+  double loop_min_cond = 0;   // smallest condition of the current loop so far
   double result[2] = {0, 0};
   int error_code = 0;  // a request that failed keeps its error; others go on
   std::string error;
@@ -63,6 +69,13 @@ struct Server {
   // after the iteration limit depend on every rounding of the earlier steps,
   // so only the complex128 run reproduces the plain path's value.
   bool escalate = false;
+  // Escalate only when the non-converging loop's smallest condition is above
+  // this (0: every non-converging loop).  A loop whose messages settled to a
+  // small but non-zero change per sweep (a slow approach or a small limit
+  // cycle) leaves them well determined, and rounding is not amplified; a
+  // loop whose messages keep changing by O(1) per sweep is the
+  // ill-conditioned case.
+  double escalate_min_cond = 0;
   int max_active;
   cudaStream_t stream = nullptr;
   double* hcond = nullptr;
