@@ -70,6 +70,10 @@ METRIC = "estimator solves/s (mixed path; plain FP64 GPU path and |dE| beside)"
 def workload_config(theta_h, world):
     return {"workload": f"kicked-Ising {L_SIDE}x{L_SIDE} open PEPS, {STEPS} steps, chi={CHI}, RZZ(-pi/4), RX(theta_h)",
             "theta_h": theta_h, "seed": SEED, "bp_tol": BP_TOL, "bp_max_iter": BP_MAXIT,
+            # the mixed path's BP loop stops at max(bp_tol, 1e-7), its rounding
+            # floor, or at the first growing condition below 1e-5; the plain
+            # path keeps bp_tol
+            "bp_tol_effective_mixed": max(BP_TOL, 1e-7),
             "sv_min": SV_MIN, "observable": f"(1/{L_SIDE * L_SIDE}) sum Z_i + 32 NN ZZ",
             "parallelism": f"replicas x{world}",
             "l2": "no flush: site tensors at BP time (~3 GB) exceed the 126 MB L2"}
