@@ -9,7 +9,8 @@ by ~3e-4.  A mixed server with escalation on restarts such a request in
 complex128, so its result is the plain path's (1e-10); a request that
 converges stays on the mixed path (1e-6).  A non-converging request whose
 value the rounding does not move (8x8, chi 16, 8 steps) stays within 1e-6
-on the mixed path itself.
+on the mixed path itself.  With an escalation threshold, only requests with
+a BP loop whose condition never came below it are restarted.
 """
 import math
 
@@ -68,10 +69,11 @@ def plain(req, precision):
     return total, conv
 
 
-def serve(reqs, escalate):
+def serve(reqs, escalate, threshold=0.0):
     srv = tb.Server(tb.MIXED, 0, 8)
     try:
         srv.set_escalation(escalate)
+        srv.set_escalation_threshold(threshold)
         ids = [srv.submit_kicked_ising(L, chi, n, THETA_J, th, observable(L, seed)) for L, chi, n, th, seed in reqs]
         steps = 0
         while any(srv.result(i) is None for i in ids):
@@ -81,6 +83,10 @@ def serve(reqs, escalate):
         return [srv.result(i) for i in ids], [srv.info(i) for i in ids]
     finally:
         srv.close()
+
+
+def _run(info):
+    return {k: info[k] for k in ("precision", "escalated", "bp_converged")}
 
 
 def _need_gpu():
@@ -94,8 +100,9 @@ def test_escalated_request_equals_the_plain_path():
     p_conv, conv_conv = plain(CONV, tb.C128)
     assert not conv_non and conv_conv
     (v_non, v_conv), (i_non, i_conv) = serve([NONCONV, CONV], escalate=True)
-    assert i_non == {"precision": tb.C128, "escalated": True, "bp_converged": False}
-    assert i_conv == {"precision": tb.MIXED, "escalated": False, "bp_converged": True}
+    assert _run(i_non) == {"precision": tb.C128, "escalated": True, "bp_converged": False}
+    assert _run(i_conv) == {"precision": tb.MIXED, "escalated": False, "bp_converged": True}
+    assert i_conv["unconverged_loops"] == 0 and i_conv["worst_min_cond"] == 0.0
     assert abs(v_non - p_non) <= TOL_PLAIN, (v_non, p_non)
     assert abs(v_conv - p_conv) <= TOL_MIXED, (v_conv, p_conv)
 
@@ -103,7 +110,8 @@ def test_escalated_request_equals_the_plain_path():
 def test_without_escalation_the_request_is_flagged_and_stays_mixed():
     _need_gpu()
     (v_non,), (i_non,) = serve([NONCONV], escalate=False)
-    assert i_non == {"precision": tb.MIXED, "escalated": False, "bp_converged": False}
+    assert _run(i_non) == {"precision": tb.MIXED, "escalated": False, "bp_converged": False}
+    assert i_non["unconverged_loops"] >= 1 and i_non["worst_final_cond"] >= i_non["worst_min_cond"] > 0
     assert math.isfinite(v_non.real) and math.isfinite(v_non.imag)
 
 
@@ -113,3 +121,22 @@ def test_nonconverging_request_within_1e6_on_the_mixed_path():
     m, conv_m = plain(NONCONV_OK, tb.MIXED)
     assert not conv_p and not conv_m
     assert abs(m - p) <= TOL_MIXED, (m, p)
+
+
+def test_escalation_threshold_picks_the_ill_conditioned_loops():
+    """With a threshold, only requests with a BP loop whose condition never
+    fell below it are restarted (tnbp_server_set_escalation_threshold): the
+    escalated set is exactly the one the non-escalating run's statistics
+    name, and every value is within the mixed tolerance of the plain path
+    (the escalated ones within the plain tolerance)."""
+    _need_gpu()
+    reqs = [NONCONV, NONCONV_OK, CONV]
+    thr = 1e-2
+    _, infos = serve(reqs, escalate=False)
+    want = [i["worst_min_cond"] > thr for i in infos]
+    assert want[0] and not want[2]
+    vals, infos_e = serve(reqs, escalate=True, threshold=thr)
+    assert [i["escalated"] for i in infos_e] == want
+    for req, v, esc in zip(reqs, vals, want):
+        p, _ = plain(req, tb.C128)
+        assert abs(v - p) <= (TOL_PLAIN if esc else TOL_MIXED), (req, v, p)

@@ -32,7 +32,6 @@
 #include "tc_leg.cuh"
 #include "tc_leg_bulk.cuh"
 #include "tc_gram.cuh"
-#include "tc_gram_persist.cuh"
 #include "tc_leg64.cuh"
 #include "tc_leg_gram.cuh"
 #include "trace.h"
@@ -1062,15 +1061,8 @@ static int launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
         break;
       }
       case SweepLaunch::GRAM_TC:
-        if (gram_persist_enabled()) {
-          // persistent: one 256-thread CTA per SM (about 194 KB of shared memory)
-          const long long grid = std::min<long long>(L.nblocks, num_sms());
-          k_gram_tc_persist<<<(unsigned)grid, 256, tc::gram_persist_smem_bytes(), stream>>>(
-              static_cast<const GramTask*>(tasks), begins, L.ntask, L.nblocks);
-        } else {
-          k_gram_tc<<<(unsigned)L.nblocks, 256, tc::gram_smem_bytes(), stream>>>(
-              static_cast<const GramTask*>(tasks), begins, L.ntask);
-        }
+        k_gram_tc<<<(unsigned)L.nblocks, 256, tc::gram_smem_bytes(), stream>>>(
+            static_cast<const GramTask*>(tasks), begins, L.ntask);
         break;
       case SweepLaunch::GRAM_T64:
         k_gram_tc64<<<(unsigned)L.nblocks, 256, tc::gram64_smem_bytes(), stream>>>(
@@ -1118,8 +1110,6 @@ static void tc_attr() {
                           (int)tc::leg_gram_smem_bytes()));
   if (!attr_done(gram_flags)) {
     CK(cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::gram_smem_bytes()));
-    CK(cudaFuncSetAttribute(k_gram_tc_persist, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)tc::gram_persist_smem_bytes()));
     CK(cudaFuncSetAttribute(k_gram_tc64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)tc::gram64_smem_bytes()));
     attr_mark(gram_flags);
@@ -1181,18 +1171,6 @@ bool bulk_leg_enabled() {
 bool leg_gram_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("TNBP_LEG_GRAM");
-    return e && e[0] == '1';
-  }();
-  return on;
-}
-
-// TNBP_GRAM_PERSIST=1 runs the complex64 Grams with C <= 32 on the
-// persistent kernel (k_gram_tc_persist: one CTA per SM, loads two 128-row
-// tiles ahead); by default on k_gram_tc (one CTA per chunk).  Both give the
-// same bits.
-bool gram_persist_enabled() {
-  static const bool on = [] {
-    const char* e = std::getenv("TNBP_GRAM_PERSIST");
     return e && e[0] == '1';
   }();
   return on;

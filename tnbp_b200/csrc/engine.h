@@ -149,7 +149,6 @@ bool autotune_enabled();
 bool tcgen05_enabled();
 bool bulk_leg_enabled();
 bool leg_gram_enabled();
-bool gram_persist_enabled();
 int num_sms();
 void check_tc_error(cudaStream_t stream);
 
