@@ -502,6 +502,9 @@ def config5_summary(tb, chi=16, steps=24, theta_h=0.6):
     res["footprint_by_chi"] = fits
     res["workload"] = (f"kicked-Ising 32x32, {steps} steps, theta_J=-pi/4, theta_h={theta_h}, chi={chi} "
                        "(stated chi 64 does not fit one GPU), 1024 Z + 1984 ZZ terms; host wall clock per solve")
+    # the first BP loop of a shape class runs the wave-budget autotuner
+    # inside the solve unless TNBP_AUTOTUNE=0 (one wave, its usual choice)
+    res["autotuner_in_solve"] = os.environ.get("TNBP_AUTOTUNE", "1") != "0"
     return res
 
 
@@ -794,6 +797,8 @@ def main():
                     help="run only the served leg and print its summary as one JSON line")
     ap.add_argument("--config5", action="store_true",
                     help="also run the 32x32 large solve at chi 16 (both paths; several minutes)")
+    ap.add_argument("--config5-only", action="store_true",
+                    help="run only the 32x32 large solve at chi 16 and print its summary as one JSON line")
     ap.add_argument("--lattice", type=int, default=L_SIDE,
                     help="lattice side (default 16; smaller sides are for profiling captures only)")
     ap.add_argument("--nsteps", type=int, default=STEPS,
@@ -803,7 +808,11 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.served_only:
+    if args.config5_only:
+        import tnbp_b200 as tb
+        if rank == 0:
+            print(json.dumps({"config5_reduced": config5_summary(tb)}))
+    elif args.served_only:
         import tnbp_b200 as tb
         if rank == 0:
             print(json.dumps({"served": served_summary(tb, args.served_requests)}))
