@@ -320,6 +320,7 @@ SweepBatch& SweepBatch::operator=(SweepBatch&& o) noexcept {
     cond = std::move(o.cond);
     launches = std::move(o.launches);
     nkernels = o.nkernels;
+    uses = o.uses;
     graph = o.graph;
     o.graph = nullptr;
   }
@@ -863,8 +864,9 @@ void Job::build_plan() {
   static std::atomic<uint64_t> serials{0};
   plan_serial = ++serials;
   // the per-job launch sequences (plan.single) are built on first use: a
-  // served job only ever runs inside batches
-  CK(cudaStreamSynchronize(stream));
+  // served job only ever runs inside batches.  Every allocation above is
+  // stream-ordered and every upload is staged before it returns, so no
+  // synchronization is needed here.
   check_budget();
 }
 
@@ -1189,11 +1191,30 @@ void check_tc_error(cudaStream_t stream) {
   }
 }
 
+// A sweep's launch sequence (one per message-arena parity) runs kernel by
+// kernel on its first kEagerSweeps uses and is captured as a CUDA graph on
+// the next, then relaunched as that graph.  Shapes change at every AbsorbTPO
+// and truncation, so a plan lives for one BP loop: on small lattices (the
+// random-circuit workload's BP at D <= 4, two or three sweeps per loop)
+// capturing both parities at once cost more host time (about 0.3 ms per
+// capture) than the sweeps themselves.
+constexpr int kEagerSweeps = 2;
+
 void Job::run_sweep(int par) {
   sync_shadow();
   if (!plan.valid) build_plan();
   SweepBatch& b = plan.single[par];
   if (b.launches.empty()) build_batch({{this, par}}, b, stream);
+  if (!b.graph && b.uses < kEagerSweeps) {
+    prepare_kernels(prec);
+    CK(cudaEventRecord(ev0, stream));
+    note_launch(launch_batch(b, prec, stream));
+    CK(cudaEventRecord(ev1, stream));
+    ++b.uses;
+    last_par = par;
+    sweeps_run++;
+    return;
+  }
   if (!b.graph) {
     TNBP_TRACE_SCOPE("sweep.graph_capture");
     prepare_kernels(prec);
@@ -1213,6 +1234,7 @@ void Job::run_sweep(int par) {
   CK(cudaGraphLaunch(b.graph, stream));
   note_launch(b.nkernels);
   CK(cudaEventRecord(ev1, stream));
+  ++b.uses;
   last_par = par;
   sweeps_run++;
 }
@@ -1573,7 +1595,9 @@ void Job::truncate(int chi_max, double sv_min, int32_t* dims_out, double* err_ou
   plan.valid = false;
   destroy_graphs();
   plan = SweepPlan();
-  CK(cudaStreamSynchronize(stream));
+  // no synchronization: the kept dims and errors are already on the host,
+  // the buffers above are freed in stream order and the uploads were staged
+  // before they returned, so the host goes on while the projectors run
   if (dims_out) for (int e = 0; e < ne; ++e) dims_out[e] = hkeep[e];
   if (err_out) for (int e = 0; e < ne; ++e) err_out[e] = herr[e];
   int bad = 0, nonfinite = 0;

@@ -101,6 +101,7 @@ struct SweepBatch {
   DevBuf arena, cond;
   std::vector<SweepLaunch> launches;
   int nkernels = 0;
+  int uses = 0;  // launches of this sequence so far (eager or graph)
   cudaGraphExec_t graph = nullptr;
   SweepBatch() = default;
   SweepBatch(const SweepBatch&) = delete;
