@@ -34,6 +34,7 @@
 #include "tc_gram.cuh"
 #include "tc_leg64.cuh"
 #include "tc_leg_gram.cuh"
+#include "site_sweep.cuh"
 #include "trace.h"
 #include "truncate.cuh"
 
@@ -665,8 +666,13 @@ void Job::build_plan() {
   // 1. each site's tree, split into its units
   std::vector<std::vector<int>> result(ns);
   std::vector<Unit> units;
+  std::vector<int> small_sites;
   for (int s = 0; s < ns; ++s) {
     const int gs = (int)g.legs[s].size();
+    if (site_whole(s)) {
+      small_sites.push_back(s);
+      continue;
+    }
     std::vector<PlanOp> ops;
     SitePlanner sp;
     sp.site = s;
@@ -841,6 +847,27 @@ void Job::build_plan() {
   // worth of partials is enough
   plan.partial.alloc(max_part * sizeof(double2), stream);
   plan.dist.alloc(std::max<size_t>(2 * ne, 1) * sizeof(double), stream);
+  for (int par = 0; par < 2; ++par) plan.site[par].clear();
+  for (int s : small_sites) {
+    const auto sh = site_shape(s);
+    const int gs = (int)g.legs[s].size();
+    for (int par = 0; par < 2; ++par) {
+      SiteTask st{};
+      st.V = sweep_vptr(s);
+      st.g = gs;
+      st.d = pd[s];
+      st.n = (int)site_elems(s);
+      for (int k = 0; k < gs; ++k) {
+        const int mo = g.out_msg(s, k);
+        st.D[k] = sh[k];
+        st.E[k] = mptr(par, g.in_msg(s, k));
+        st.out[k] = mptr(1 - par, mo);
+        st.old[k] = mptr(par, mo);
+        st.dist[k] = static_cast<double*>(plan.dist.p) + mo;
+      }
+      plan.site[par].push_back(st);
+    }
+  }
   double2* partial = static_cast<double2*>(plan.partial.p);
   for (size_t i = 0; i < plan.gram.size(); ++i) plan.gram[i].partial = partial + pend[gram_part[i]].part_off;
   for (size_t i = 0; i < lg_part.size(); ++i)
@@ -908,6 +935,17 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
   // shares the batch.  A request's rounding therefore does not depend on
   // what it is batched with.
   const bool tc_ok = !entries.empty() && reduced_sweeps(entries[0].job->prec) && tcgen05_enabled();
+  {
+    // small sites: one CTA each, every message of the site on chip
+    std::vector<SiteTask> sts;
+    size_t smem = 0;
+    for (auto& e : entries)
+      for (const SiteTask& st : e.job->plan.site[e.parity]) {
+        sts.push_back(st);
+        smem = std::max(smem, site_sweep_smem_bytes(st.D, st.g, st.d));
+      }
+    add(SweepLaunch::SITE, sts, {}, (long long)sts.size(), (int)smem);
+  }
   for (size_t w = 0; w < nw; ++w) {
     size_t nlev = 0;
     for (auto& e : entries)
@@ -1002,7 +1040,7 @@ void build_batch(const std::vector<BatchEntry>& entries, SweepBatch& b, cudaStre
     const auto& P = entries[ei].job->plan;
     SumTask s1;
     s1.x = static_cast<const double*>(P.dist.p);
-    s1.n = (int)P.msg[0].size();
+    s1.n = (int)(2 * entries[ei].job->g.edges.size());  // every message's distance
     s1.scale = 1.0 / (2.0 * (double)entries[ei].job->g.edges.size());
     s1.out = static_cast<double*>(b.cond.p) + ei;
     st.push_back(s1);
@@ -1025,6 +1063,7 @@ static void leg_apply_attr() {
   std::lock_guard<std::mutex> lk(g_attr_mu);
   if (attr_done(flags)) return;
   CK(cudaFuncSetAttribute(k_leg_apply<R, MR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)leg_smem<R>(128)));
+  CK(cudaFuncSetAttribute(k_site_sweep<R, MR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSiteSmemMax));
   attr_mark(flags);
 }
 
@@ -1079,6 +1118,9 @@ static int launch_batch_t(const SweepBatch& b, cudaStream_t stream) {
         break;
       case SweepLaunch::MSG:
         k_msg_finalize<R, MR><<<L.ntask, kThreads, 0, stream>>>(static_cast<const MsgTask*>(tasks));
+        break;
+      case SweepLaunch::SITE:  // max_din holds the launch's shared memory bytes
+        k_site_sweep<R, MR><<<L.ntask, kThreads, (size_t)L.max_din, stream>>>(static_cast<const SiteTask*>(tasks));
         break;
       case SweepLaunch::SUM:
         k_segmented_sum<<<L.ntask, kThreads, 0, stream>>>(static_cast<const SumTask*>(tasks));
@@ -1176,6 +1218,25 @@ bool leg_gram_enabled() {
     return e && e[0] == '1';
   }();
   return on;
+}
+
+// TNBP_SITE_SWEEP=1 sweeps every site whose tensor, two work buffers,
+// messages and Gram partials fit kSiteSmemMax of shared memory in one CTA
+// (k_site_sweep); other sites, and every site by default, take the
+// per-level path.
+bool site_sweep_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("TNBP_SITE_SWEEP");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+bool Job::site_whole(int s) const {
+  const int gs = (int)g.legs[s].size();
+  if (!site_sweep_enabled() || gs < 1 || gs > kMaxLegs) return false;
+  const auto sh = site_shape(s);
+  return site_sweep_smem_bytes(sh.data(), gs, pd[s]) <= kSiteSmemMax;
 }
 
 // A tcgen05 CTA that gave up waiting for its MMAs records it in g_tc_error.

@@ -86,7 +86,7 @@ struct WaveHost {
 // One kernel launch of a sweep batch; its task arrays live in the batch's
 // arena at the given byte offsets.
 struct SweepLaunch {
-  enum Kind { LEG_BULK, LEG_T64, LEG_TC, LEG_CORE, GRAM_TC, GRAM_T64, GRAM_CORE, LEG_GRAM, MSG, SUM };
+  enum Kind { LEG_BULK, LEG_T64, LEG_TC, LEG_CORE, GRAM_TC, GRAM_T64, GRAM_CORE, LEG_GRAM, MSG, SUM, SITE };
   int kind;
   size_t tasks_off, begins_off;
   int ntask;
@@ -121,6 +121,7 @@ struct SweepPlan {
   std::vector<long long> gram_blocks;  // blocks of each gram task (CUDA-core kernel)
   std::vector<LegGramTask> lg[2];      // fused last absorption + Gram, per parity
   std::vector<MsgTask> msg[2];         // one per target, per message-arena parity
+  std::vector<SiteTask> site[2];       // sites swept whole on chip (k_site_sweep), per parity
   SweepBatch single[2];
   double flops = 0.0, bytes_alg = 0.0;
   SweepPlan() = default;
@@ -150,6 +151,7 @@ bool autotune_enabled();
 bool tcgen05_enabled();
 bool bulk_leg_enabled();
 bool leg_gram_enabled();
+bool site_sweep_enabled();
 int num_sms();
 void check_tc_error(cudaStream_t stream);
 
@@ -231,6 +233,7 @@ struct Job {
   Job(const int32_t* e, int64_t n, const int32_t* pdims, int precision, cudaStream_t s, uint64_t budget);
   ~Job();
   std::vector<int> site_shape(int s) const;
+  bool site_whole(int s) const;  // swept whole on chip by k_site_sweep
   size_t site_elems(int s) const;
   void layout();
   void put_complex(DevBuf& dst, const double* src, size_t n, size_t elem_off);

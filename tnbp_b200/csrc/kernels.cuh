@@ -225,6 +225,31 @@ struct LegGramTask {
   long long block_begin; // exclusive prefix of nchunk over tasks
 };
 
+// One small site's whole sweep (k_site_sweep, site_sweep.cuh).
+struct SiteTask {
+  const void* V;               // site tensor (R), column-major (D_0, ..., D_{g-1}, d)
+  const void* E[kMaxLegs];     // incoming message of leg k (MR), D_k x D_k
+  void* out[kMaxLegs];         // new outgoing message of leg k (MR)
+  const void* old[kMaxLegs];   // stored outgoing message of leg k (MR)
+  double* dist[kMaxLegs];      // || new/|new| - old/|old| ||_F of leg k
+  int D[kMaxLegs];
+  int g, d, n;                 // degree, physical dim, d prod D
+};
+
+// Shared memory of one site: V and two buffers of n complex FP64 values, the
+// incoming messages, and max(256, C^2) partial sums of the Gram.
+__host__ __device__ inline size_t site_sweep_smem_bytes(const int* D, int g, int d) {
+  size_t n = (size_t)d, sd2 = 0, cmax2 = 0;
+  for (int k = 0; k < g; ++k) {
+    n *= (size_t)D[k];
+    sd2 += (size_t)D[k] * D[k];
+    cmax2 = cmax2 > (size_t)D[k] * D[k] ? cmax2 : (size_t)D[k] * D[k];
+  }
+  const size_t part = cmax2 > 256 ? cmax2 : 256;
+  return 16 * (3 * n + sd2 + part);
+}
+constexpr size_t kSiteSmemMax = 160 * 1024;
+
 // ---------------------------------------------------------------------------
 // Reduce Gram partials (fixed order), normalize by the Frobenius norm
 // (bp.h:166), store the new message, and the distance to the normalized
