@@ -659,8 +659,11 @@ void Job::autotune_waves() {
 
 void Job::build_plan() {
   TNBP_TRACE_SCOPE("sweep.build_plan");
-  destroy_graphs();
-  plan = SweepPlan();
+  {
+    TNBP_TRACE_SCOPE("sweep.build_plan.release");
+    destroy_graphs();
+    plan = SweepPlan();
+  }
   const int ns = (int)g.labels.size();
   const int ne = (int)g.edges.size();
   // 1. each site's tree, split into its units
@@ -694,7 +697,11 @@ void Job::build_plan() {
   }
   // 2. waves of consecutive units within the byte budget (at least one unit)
   if (!tuning) choose_wave_budget();
-  const size_t cap = scratch_limit();
+  size_t cap = 0;
+  {
+    TNBP_TRACE_SCOPE("sweep.build_plan.scratch_limit");
+    cap = scratch_limit();
+  }
   const size_t budget = wave_budget && wave_budget < cap ? wave_budget : cap;
   std::vector<std::vector<int>> waves;
   {
@@ -725,7 +732,10 @@ void Job::build_plan() {
     }
     scratch = std::max(scratch, o);
   }
-  ws_scratch.ensure(std::max<size_t>(scratch, 32) * wsz, stream);
+  {
+    TNBP_TRACE_SCOPE("sweep.build_plan.scratch_alloc");
+    ws_scratch.ensure(std::max<size_t>(scratch, 32) * wsz, stream);
+  }
   auto slot_ptr = [&](int ui, int slot) -> void* {
     const Unit& U = units[ui];
     if (slot < 0) return sweep_vptr(U.site);
