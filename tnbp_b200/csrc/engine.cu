@@ -159,6 +159,41 @@ int Graph::in_msg(int s, int k) const {
   return site_a[e] == s ? e + (int)edges.size() : e;
 }
 
+// Page-locked 64-byte slots for the jobs' condition read-backs.  A
+// cudaMallocHost and cudaFreeHost per job cost milliseconds (page locking,
+// and the free synchronizes the device): a job takes a slot from blocks
+// allocated once per process and gives it back when it is destroyed (after
+// its stream is idle, so no copy into the slot is pending).
+namespace {
+struct PinnedSlots {
+  std::mutex mu;
+  std::vector<double*> free;
+};
+PinnedSlots& pinned_slots() {
+  static PinnedSlots* p = new PinnedSlots();  // blocks live until exit
+  return *p;
+}
+constexpr size_t kSlotBytes = 64, kSlotsPerBlock = 1024;
+double* pinned_slot_get() {
+  PinnedSlots& P = pinned_slots();
+  std::lock_guard<std::mutex> lk(P.mu);
+  if (P.free.empty()) {
+    void* b = nullptr;
+    CK(cudaMallocHost(&b, kSlotBytes * kSlotsPerBlock));
+    for (size_t i = kSlotsPerBlock; i-- > 0;)
+      P.free.push_back(reinterpret_cast<double*>(static_cast<char*>(b) + i * kSlotBytes));
+  }
+  double* slot = P.free.back();
+  P.free.pop_back();
+  return slot;
+}
+void pinned_slot_put(double* slot) {
+  PinnedSlots& P = pinned_slots();
+  std::lock_guard<std::mutex> lk(P.mu);
+  P.free.push_back(slot);
+}
+}  // namespace
+
 // -------------------------------------------------------------------- job
 Job::Job(const int32_t* e, int64_t n, const int32_t* pdims, int precision, cudaStream_t s,
          uint64_t budget)
@@ -182,7 +217,7 @@ Job::Job(const int32_t* e, int64_t n, const int32_t* pdims, int precision, cudaS
   }
   CK(cudaEventCreate(&ev0));
   CK(cudaEventCreate(&ev1));
-  CK(cudaMallocHost(&host_scalar, 64));
+  host_scalar = pinned_slot_get();
   const int ns = (int)g.labels.size();
   pd.assign(ns, 2);
   if (pdims) for (int i = 0; i < ns; ++i) pd[i] = pdims[i];
@@ -208,7 +243,7 @@ Job::~Job() {
   V.release(); M[0].release(); M[1].release(); V32.release();
   ws_scratch.release(); ws_chain[0].release(); ws_chain[1].release(); Vspare.release();
   plan = SweepPlan();
-  if (host_scalar) cudaFreeHost(host_scalar);
+  if (host_scalar) pinned_slot_put(host_scalar);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   cudaStreamSynchronize(stream);
