@@ -1,7 +1,8 @@
 """The site-resident sweep kernel (k_site_sweep) against the numpy oracle.
 
-With TNBP_SITE_SWEEP=1 every site whose tensor, work buffers, messages and
-Gram partials fit the kernel's shared memory is swept whole by one CTA (every
+By default (TNBP_SITE_SWEEP=0 turns it off) every site whose tensor, work
+buffers, messages and Gram partials fit the kernel's shared memory is swept
+whole by one CTA (every
 outgoing message, its normalization and its distance to the stored message),
 the other sites by the per-level kernels in the same sweep.  Each case runs
 in its own process (the switch is read once per process): one sweep of
