@@ -248,7 +248,10 @@ __host__ __device__ inline size_t site_sweep_smem_bytes(const int* D, int g, int
   const size_t part = cmax2 > 256 ? cmax2 : 256;
   return 16 * (3 * n + sd2 + part);
 }
-constexpr size_t kSiteSmemMax = 160 * 1024;
+// Sites up to 64 KB (1024 elements at degree 3 and 4: D <= 8 and D <= 4) are
+// swept whole; larger ones (a degree-2 corner at D = 32 would take 147 KB and
+// one CTA per SM) measured faster on the per-level tcgen05 path.
+constexpr size_t kSiteSmemMax = 64 * 1024;
 
 // ---------------------------------------------------------------------------
 // Reduce Gram partials (fixed order), normalize by the Frobenius norm
