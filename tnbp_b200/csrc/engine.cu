@@ -14,6 +14,7 @@
 #include <cmath>
 #include <complex>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -669,6 +670,15 @@ static bool wave_budget_fixed() {
 // kept in a table per device (name and SM count) in $TNBP_TUNE_DIR (default
 // $HOME/.cache/tnbp_b200), one line per class: class, budget in MiB, best
 // and default sweep ms.  TNBP_AUTOTUNE=0 turns the tuner off.
+// TNBP_TUNE_LOG=1 prints every candidate's timing to stderr.
+static bool tune_log_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("TNBP_TUNE_LOG");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
 bool autotune_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("TNBP_AUTOTUNE");
@@ -782,6 +792,9 @@ void Job::autotune_waves() {
     }
     if (reduced_sweeps(prec)) check_tc_error(stream);
     ms /= 2.0;
+    if (tune_log_enabled())
+      std::fprintf(stderr, "tnbp autotune %s: wave budget %zu MiB (0 = one wave), %zu waves, %.3f ms per sweep\n",
+                   key.c_str(), mb, plan.waves.size(), ms);
     if (mb == (wave_budget_bytes() >> 20)) default_ms = ms;
     // a later (smaller) budget must be 3 % faster to replace an earlier one:
     // two timed sweeps do not resolve smaller differences
