@@ -126,9 +126,20 @@ size_t cached_device_bytes(int dev) {
 DevBuf::~DevBuf() { release(); }
 void DevBuf::release() {
   if (p) {
-    int dev = 0;
+    // work on the buffer's own device (a job may be released while another
+    // device is current)
+    int cur = -1;
+    const bool switched = dev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != dev &&
+                          cudaSetDevice(dev) == cudaSuccess;
+    struct Restore {
+      bool on;
+      int d;
+      ~Restore() {
+        if (on) cudaSetDevice(d);
+      }
+    } restore{switched, cur};
     cudaEvent_t ev = nullptr;
-    if (bytes >= kCacheMinBytes && cudaGetDevice(&dev) == cudaSuccess &&
+    if (bytes >= kCacheMinBytes && dev >= 0 &&
         cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess && cudaEventRecord(ev, stream) == cudaSuccess) {
       BlockCache& C = block_cache();
       std::lock_guard<std::mutex> lk(C.mu);
@@ -159,9 +170,10 @@ void DevBuf::release() {
 void DevBuf::alloc(size_t nbytes, cudaStream_t s) {
   release();
   stream = s;
+  dev = -1;
   if (nbytes == 0) return;
-  int dev = 0;
   const bool have_dev = cudaGetDevice(&dev) == cudaSuccess;
+  if (!have_dev) dev = -1;
   if (nbytes >= kCacheMinBytes && have_dev) {
     BlockCache& C = block_cache();
     std::lock_guard<std::mutex> lk(C.mu);
