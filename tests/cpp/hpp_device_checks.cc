@@ -1,6 +1,8 @@
 // Device checks of include/tnbp_b200.hpp: the estimator loop through the
 // C++ interface (State) and the same program served (Server) give the same
-// sum_k c_k <P_k>; a cancelled request throws; checkpoint round trip.
+// sum_k c_k <P_k>; a cancelled request throws; checkpoint round trip; a mixed
+// server with an escalation threshold reports its request's run and BP
+// statistics and stays within 1e-6.
 // usage: hpp_device_checks <program.qasm> <observable.txt> <chi> <tol> <maxit> <sv_min> <scratch file>
 #include <cstdio>
 #include <cstdlib>
@@ -58,7 +60,30 @@ int main(int argc, char** argv) {
     }
     std::printf("direct %.17g %.17g served %.17g %.17g reloaded %.17g cancelled %d\n", direct.real(), direct.imag(),
                 served.real(), served.imag(), reloaded.real(), (int)cancelled);
-    const bool ok = std::abs(direct - served) <= 1e-10 && direct == reloaded && cancelled;
+    // a mixed server with escalation and a threshold: the request's run
+    // fields and BP statistics come back through the C++ interface
+    tb::Server msrv(TNBP_MIXED, 0, 2);
+    msrv.set_escalation(true);
+    msrv.set_escalation_threshold(1e-2);
+    bool bad_threshold = false;
+    try {
+      msrv.set_escalation_threshold(-1.0);
+    } catch (const std::invalid_argument&) {
+      bad_threshold = true;
+    }
+    const int64_t m = msrv.submit_qasm(qasm, pauli, chi, tol, maxit, sv_min);
+    tb::cplx mixed;
+    steps = 0;
+    while (!msrv.result(m, &mixed) && steps < 100000) { msrv.step(); ++steps; }
+    const auto inf = msrv.info(m);
+    std::printf("mixed %.17g %.17g precision %d escalated %d converged %d loops %d min %.3g final %.3g bad %d\n",
+                mixed.real(), mixed.imag(), inf.precision, (int)inf.escalated, (int)inf.bp_converged,
+                inf.unconverged_loops, inf.worst_min_cond, inf.worst_final_cond, (int)bad_threshold);
+    const bool info_ok = bad_threshold && inf.unconverged_loops >= 0 && inf.worst_final_cond >= inf.worst_min_cond &&
+                         (inf.bp_converged == (inf.unconverged_loops == 0)) &&
+                         (inf.escalated ? inf.precision == TNBP_C128 : inf.precision == TNBP_MIXED);
+    const bool ok = std::abs(direct - served) <= 1e-10 && direct == reloaded && cancelled && info_ok &&
+                    std::abs(mixed - direct) <= 1e-6;
     return ok ? 0 : 1;
   } catch (const std::exception& e) {
     std::printf("exception: %s\n", e.what());
