@@ -41,6 +41,9 @@ Server::Server(int precision, uint64_t budget_bytes, int max_active_jobs)
   }
   keep_pool_memory();
   CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
   if (budget == 0) {
     const size_t fr = device_bytes_available();
     const size_t reserve = (size_t)4 << 30;
@@ -52,8 +55,12 @@ Server::~Server() {
   sweeps.clear();
   for (auto& kv : reqs) { kv.second->job.reset(); kv.second->tpos.reset(); }
   tpo_cache.clear();
-  if (hcond) cudaFreeHost(hcond);
+  for (auto& h : hconds)
+    if (h.p) cudaFreeHost(h.p);
+  if (stream2) { cudaStreamSynchronize(stream2); cudaStreamDestroy(stream2); }
   if (stream) { cudaStreamSynchronize(stream); cudaStreamDestroy(stream); }
+  if (ev_fork) cudaEventDestroy(ev_fork);
+  if (ev_join) cudaEventDestroy(ev_join);
 }
 
 // Sweep scratch slots of a degree-g site under the tree schedule of
@@ -272,10 +279,15 @@ void Server::restart_c128(Request& r) {
   start(r);
 }
 
-// One batched BP sweep over the requests of `grp`, whose jobs all have
-// precision gprec, and the BP-loop decision of each request.
-void Server::sweep_group(int gprec, const std::vector<Request*>& inbp) {
+// The batched BP sweep of one group of requests whose jobs all have
+// precision gprec: its task arrays built (on the server's stream, where the
+// jobs' own work runs) and, once launched, its read-back and the BP-loop
+// decision of each request.
+Server::GroupSweep Server::prepare_group(int gprec, const std::vector<Request*>& inbp) {
   TNBP_TRACE_SCOPE("server.3_sweep");
+  GroupSweep g;
+  g.gprec = gprec;
+  g.reqs = inbp;
   std::vector<BatchEntry> entries;
   for (auto* r : inbp) {
     r->job->sync_shadow();
@@ -292,6 +304,10 @@ void Server::sweep_group(int gprec, const std::vector<Request*>& inbp) {
     it = sweeps.emplace(key, std::move(cs)).first;
     sweeps_lru.push_back(key);
     while (sweeps.size() > sweeps_cap) {
+      if (sweeps_lru.front() == key) {  // never the batch about to run
+        sweeps_lru.splice(sweeps_lru.end(), sweeps_lru, sweeps_lru.begin());
+        continue;
+      }
       sweeps.erase(sweeps_lru.front());
       sweeps_lru.pop_front();
     }
@@ -299,55 +315,67 @@ void Server::sweep_group(int gprec, const std::vector<Request*>& inbp) {
     sweeps_lru.remove(key);
     sweeps_lru.push_back(key);
   }
-  CachedSweep& cs = *it->second;
+  g.cs = it->second.get();
+  return g;
+}
+
+// Launches a prepared group on stream s (captured as a CUDA graph on its
+// second use, relaunched as that graph after) and queues the read-back of
+// its conditions into the pinned buffer h.
+void Server::launch_group(GroupSweep& g, cudaStream_t s, PinnedConds& h) {
+  CachedSweep& cs = *g.cs;
   SweepBatch& batch = cs.batch;
   if (cs.uses == 1 && !batch.graph) {
     TNBP_TRACE_SCOPE("server.3_graph_capture");
     cudaGraph_t graph;
-    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try {
-      batch.nkernels = launch_batch(batch, gprec, stream);
+      batch.nkernels = launch_batch(batch, g.gprec, s);
     } catch (...) {
-      cudaStreamEndCapture(stream, &graph);
+      cudaStreamEndCapture(s, &graph);
       throw;
     }
-    CK(cudaStreamEndCapture(stream, &graph));
+    CK(cudaStreamEndCapture(s, &graph));
     CK(cudaGraphInstantiate(&batch.graph, graph, 0));
     cudaGraphDestroy(graph);
   }
   if (batch.graph) {
-    CK(cudaGraphLaunch(batch.graph, stream));
+    CK(cudaGraphLaunch(batch.graph, s));
     note_launch(batch.nkernels);
     ++graph_launches;
   } else {
-    note_launch(launch_batch(batch, gprec, stream));
+    note_launch(launch_batch(batch, g.gprec, s));
     ++eager_launches;
   }
   ++cs.uses;
-  if (hcond_cap < entries.size()) {
-    if (hcond) cudaFreeHost(hcond);
-    hcond_cap = std::max<size_t>(64, 2 * entries.size());
-    CK(cudaMallocHost(&hcond, hcond_cap * sizeof(double)));
+  if (h.cap < g.reqs.size()) {
+    if (h.p) cudaFreeHost(h.p);
+    h.p = nullptr;
+    h.cap = std::max<size_t>(64, 2 * g.reqs.size());
+    CK(cudaMallocHost(&h.p, h.cap * sizeof(double)));
   }
-  CK(cudaMemcpyAsync(hcond, batch.cond.p, entries.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
-  CK(cudaStreamSynchronize(stream));
-  if (reduced_sweeps(gprec)) check_tc_error(stream);
-  for (size_t i = 0; i < inbp.size(); ++i) {
-    Request& r = *inbp[i];
+  g.h = h.p;
+  CK(cudaMemcpyAsync(h.p, batch.cond.p, g.reqs.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+}
+
+// After the group's stream has finished: each request's BP-loop decision.
+void Server::finish_group(GroupSweep& g) {
+  for (size_t i = 0; i < g.reqs.size(); ++i) {
+    Request& r = *g.reqs[i];
     Job& j = *r.job;
     if (r.bp_iters == 0) {  // first sweep of the loop: always kept
       j.cur = 1 - j.cur;
       r.bp_iters = 1;
       continue;
     }
-    const double c = hcond[i];
+    const double c = g.h[i];
     if (!std::isfinite(c)) {
       fail(r, TNBP_ENOTCONV, "BP condition is not finite (non-finite messages)");
       continue;
     }
-    const bool conv = c < effective_tol(gprec, r.tol);
+    const bool conv = c < effective_tol(g.gprec, r.tol);
     r.loop_min_cond = std::min(r.loop_min_cond, c);
-    if (conv || r.bp_iters >= r.maxit || stop_on_growth(gprec, r.prev_cond, c)) {
+    if (conv || r.bp_iters >= r.maxit || stop_on_growth(g.gprec, r.prev_cond, c)) {
       r.phase = Request::TRUNC;  // keep the current messages
       if (!conv && r.bp_iters >= r.maxit) {
         r.bp_converged = false;
@@ -390,15 +418,36 @@ void Server::step(int* n_active, int* n_queued, int* n_done) {
     }
   }
   // 3. one batched BP sweep over every request in its BP phase, one batch
-  // per job precision (requests escalated to complex128 sweep apart)
+  // per job precision.  Requests escalated to complex128 sweep apart, on a
+  // second stream forked from the server's stream before the first batch
+  // and joined back after, so the two batches can run side by side; the host
+  // waits once for both.
   {
     std::vector<Request*> grp[2];
     for (int64_t id : active) {
       Request& r = *reqs[id];
       if (r.phase == Request::BP) grp[r.prec == prec ? 0 : 1].push_back(&r);
     }
-    if (!grp[0].empty()) sweep_group(prec, grp[0]);
-    if (!grp[1].empty()) sweep_group(TNBP_C128, grp[1]);
+    std::vector<GroupSweep> gs;
+    if (!grp[0].empty()) gs.push_back(prepare_group(prec, grp[0]));
+    if (!grp[1].empty()) gs.push_back(prepare_group(TNBP_C128, grp[1]));
+    if (gs.size() == 2) CK(cudaEventRecord(ev_fork, stream));
+    for (size_t k = 0; k < gs.size(); ++k) {
+      if (k == 1) {
+        CK(cudaStreamWaitEvent(stream2, ev_fork, 0));
+        launch_group(gs[k], stream2, hconds[1]);
+        CK(cudaEventRecord(ev_join, stream2));
+        CK(cudaStreamWaitEvent(stream, ev_join, 0));
+      } else {
+        launch_group(gs[k], stream, hconds[0]);
+      }
+    }
+    if (!gs.empty()) {
+      CK(cudaStreamSynchronize(stream));
+      if (gs.size() == 2) CK(cudaStreamSynchronize(stream2));
+      if (reduced_sweeps(prec)) check_tc_error(stream);
+      for (auto& g : gs) finish_group(g);
+    }
   }
   // 4. truncation, next step or measurement
   TNBP_TRACE_SCOPE("server.4_trunc_measure");

@@ -77,9 +77,15 @@ struct Server {
   // ill-conditioned case.
   double escalate_min_cond = 0;
   int max_active;
-  cudaStream_t stream = nullptr;
-  double* hcond = nullptr;
-  size_t hcond_cap = 0;
+  cudaStream_t stream = nullptr;   // every job's own work and the server's first batch
+  cudaStream_t stream2 = nullptr;  // the complex128 batch of escalated requests
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // page-locked read-back of each batch's conditions (one per batch of a step)
+  struct PinnedConds {
+    double* p = nullptr;
+    size_t cap = 0;
+  };
+  PinnedConds hconds[2];
   int64_t next_id = 1;
   std::deque<int64_t> queue;
   std::map<int64_t, std::unique_ptr<Request>> reqs;
@@ -112,7 +118,15 @@ struct Server {
                                         const std::function<void(tnbp_host::Edges&,
                                                                  std::vector<tnbp_host::Layer>&)>& build);
   void step(int* n_active, int* n_queued, int* n_done);
-  void sweep_group(int gprec, const std::vector<Request*>& grp);
+  struct GroupSweep {
+    int gprec = 0;
+    std::vector<Request*> reqs;
+    CachedSweep* cs = nullptr;
+    double* h = nullptr;
+  };
+  GroupSweep prepare_group(int gprec, const std::vector<Request*>& grp);
+  void launch_group(GroupSweep& g, cudaStream_t s, PinnedConds& h);
+  void finish_group(GroupSweep& g);
   void restart_c128(Request& r);
   uint64_t footprint(const Request& r) const;
   void start(Request& r);
