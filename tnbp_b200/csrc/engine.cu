@@ -1593,8 +1593,14 @@ void Job::absorb_tpo(const Tpo& tpo) {
     t.g = (int)g.legs[s].size();
     t.d = pd[s];
     t.dout = tpo.dout[s];
-    for (int k = 0; k < t.g; ++k) { t.Dv[k] = odim[g.legs[s][k]]; t.r[k] = tpo.rank[g.legs[s][k]]; }
+    for (int k = 0; k < t.g; ++k) {
+      t.Dv[k] = odim[g.legs[s][k]];
+      t.r[k] = tpo.rank[g.legs[s][k]];
+      t.div_m[k] = make_fastdiv((uint32_t)(t.Dv[k] * t.r[k]));
+      t.div_v[k] = make_fastdiv((uint32_t)t.Dv[k]);
+    }
     t.n_out = (long long)site_elems(s);
+    if (t.n_out >= (1ll << 31)) throw Error(TNBP_EUNSUPPORTED, "site tensor of 2^31 or more elements");
     t.block_begin = nb;
     ab.push_back(nb);
     nb += (t.n_out + kThreads - 1) / kThreads;

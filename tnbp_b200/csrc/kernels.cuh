@@ -357,6 +357,22 @@ static __global__ void k_sum_scaled(const double* __restrict__ x, int n, double 
 //   V'[(v_0,o_0),...,(v_{g-1},o_{g-1}), p'] = sum_p O[o..., p, p'] V[v..., p]
 // merged bond index v + D*o (column-major reshape of (v, o)).
 // ---------------------------------------------------------------------------
+// Division of unsigned values below 2^31 by an invariant divisor d >= 1
+// (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994): q = (mulhi(x, m) + x) >> s with
+// s = ceil(log2 d) and m = floor(2^32 (2^s - d) / d) + 1, set up once on the
+// host.  mulhi(x, m) < x, so the sum stays below 2^32 for x < 2^31.
+struct FastDiv {
+  uint32_t d, m, s;
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+  uint32_t s = 0;
+  while ((1ull << s) < d) ++s;
+  const unsigned long long m = (((1ull << 32) * ((1ull << s) - d)) / d) + 1;
+  return FastDiv{d, (uint32_t)m, s};
+}
+__device__ __forceinline__ uint32_t fast_div(uint32_t x, const FastDiv& f) { return (__umulhi(x, f.m) + x) >> f.s; }
+
 struct AbsorbTask {
   const void* V;
   void* out;
@@ -364,7 +380,9 @@ struct AbsorbTask {
   int g, d, dout;
   int Dv[kMaxLegs];
   int r[kMaxLegs];
-  long long n_out;
+  FastDiv div_m[kMaxLegs];  // by Dv[k] r[k] (the merged bond of leg k)
+  FastDiv div_v[kMaxLegs];  // by Dv[k]
+  long long n_out;          // < 2^31 (checked on the host)
   long long block_begin;
 };
 
@@ -377,23 +395,26 @@ __global__ void __launch_bounds__(kThreads) k_absorb_sites(const AbsorbTask* __r
   const AbsorbTask& tk = tasks[ti];
   const long long i = (blockIdx.x - tk.block_begin) * kThreads + threadIdx.x;
   if (i >= tk.n_out) return;
-  long long rem = i;
-  long long voff = 0, vstride = 1, ooff = 0, ostride = 1;
+  // the output index's digits: 32-bit, divisions by the legs' invariant
+  // merged and bond dims
+  uint32_t rem = (uint32_t)i;
+  uint32_t voff = 0, vstride = 1, ooff = 0, ostride = 1;
   for (int k = 0; k < tk.g; ++k) {
-    const long long M = (long long)tk.Dv[k] * tk.r[k];
-    const long long mk = rem % M;
-    rem /= M;
-    voff += (mk % tk.Dv[k]) * vstride;
-    ooff += (mk / tk.Dv[k]) * ostride;
-    vstride *= tk.Dv[k];
-    ostride *= tk.r[k];
+    const uint32_t q = fast_div(rem, tk.div_m[k]);
+    const uint32_t mk = rem - q * tk.div_m[k].d;
+    rem = q;
+    const uint32_t o = fast_div(mk, tk.div_v[k]);
+    voff += (mk - o * tk.div_v[k].d) * vstride;
+    ooff += o * ostride;
+    vstride *= tk.div_v[k].d;
+    ostride *= (uint32_t)tk.r[k];
   }
-  const long long pout = rem;  // < dout
+  const uint32_t pout = rem;  // < dout
   const C* V = static_cast<const C*>(tk.V);
   double2 acc = make_double2(0.0, 0.0);
   for (int p = 0; p < tk.d; ++p) {
-    const double2 v = to_d2(V[voff + vstride * p]);
-    const double2 o = tk.O[ooff + ostride * (p + (long long)tk.d * pout)];
+    const double2 v = to_d2(V[voff + (size_t)vstride * p]);
+    const double2 o = tk.O[ooff + (size_t)ostride * (p + (size_t)tk.d * pout)];
     acc = acc + v * o;
   }
   static_cast<C*>(tk.out)[i] = from_d2<C>(acc);
