@@ -954,6 +954,7 @@ void Job::build_plan() {
           lt.out = slot_ptr(ui, op.dst);
           lt.mat = mptr(par, g.in_msg(op.site, op.leg));
           lt.L = L; lt.R = R; lt.Din = sh[op.leg]; lt.Dout = sh[op.leg];
+          set_leg_divisors(lt);
           lt.block_begin = 0;  // assigned when a batch is built
           W.levels[op.level].tasks[par].push_back(lt);
         }
@@ -1713,6 +1714,7 @@ void Job::run_chains(std::vector<ChainEntry>& chains) {
         lt.out = (lv + 1 == c.legs.size()) ? c.dst : static_cast<char*>(buf[lv & 1].p) + base[i - i0] * esz;
         lt.mat = c.mats[lv];
         lt.L = L; lt.R = R; lt.Din = sh[leg]; lt.Dout = c.dout[lv];
+        set_leg_divisors(lt);
         lt.block_begin = nb;
         b.push_back(nb);
         nb += (L * R + kRowTile - 1) / kRowTile;

@@ -16,6 +16,22 @@ constexpr int kColTile = 32;   // output columns per inner chunk
 constexpr int kMaxLegs = 8;    // maximum site degree supported
 constexpr int kSvdMaxSweeps = 60;
 
+// Division of unsigned values below 2^31 by an invariant divisor d >= 1
+// (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994): q = (mulhi(x, m) + x) >> s with
+// s = ceil(log2 d) and m = floor(2^32 (2^s - d) / d) + 1, set up once on the
+// host.  mulhi(x, m) < x, so the sum stays below 2^32 for x < 2^31.
+struct FastDiv {
+  uint32_t d, m, s;
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+  uint32_t s = 0;
+  while ((1ull << s) < d) ++s;
+  const unsigned long long m = (((1ull << 32) * ((1ull << s) - d)) / d) + 1;
+  return FastDiv{d, (uint32_t)m, s};
+}
+__device__ __forceinline__ uint32_t fast_div(uint32_t x, const FastDiv& f) { return (__umulhi(x, f.m) + x) >> f.s; }
+
 // ---------------------------------------------------------------------------
 // Leg contraction  out[l, k, r] = sum_j in[l, j, r] * mat[j, k]
 //   in : L x Din x R, out : L x Dout x R (column-major), mat : Din x Dout.
@@ -28,10 +44,16 @@ struct LegTask {
   const void* in;
   void* out;
   const void* mat;
-  long long L, R;
+  long long L, R;         // L R < 2^31 (a site tensor has fewer than 2^31 elements)
   int Din, Dout;
   long long block_begin;  // exclusive prefix of row tiles over tasks
+  FastDiv div_l;          // by L: the CUDA-core kernel's row split q = l + L r
+  FastDiv div_din;        // by Din
 };
+inline void set_leg_divisors(LegTask& t) {
+  t.div_l = make_fastdiv((uint32_t)t.L);
+  t.div_din = make_fastdiv((uint32_t)t.Din);
+}
 
 __device__ __forceinline__ int find_task(const long long* begins, int n, long long b) {
   int lo = 0, hi = n - 1;
@@ -72,12 +94,13 @@ __global__ void __launch_bounds__(kThreads) k_leg_apply(const LegTask* __restric
   for (int idx = threadIdx.x; idx < nA; idx += kThreads) {
     int qq, j;
     if (qfast) { qq = idx % kRowTile; j = idx / kRowTile; }
-    else { j = idx % Din; qq = idx / Din; }
+    else { qq = (int)fast_div((uint32_t)idx, tk.div_din); j = idx - qq * Din; }
     const long long q = q0 + qq;
     C v = czero<C>();
     if (q < rows) {
-      const long long l = q % L, r = q / L;
-      v = in[l + L * j + L * Din * r];
+      const uint32_t r = fast_div((uint32_t)q, tk.div_l);
+      const long long l = (long long)((uint32_t)q - r * (uint32_t)L);
+      v = in[l + L * j + L * Din * (long long)r];
     }
     As[qq * ldA + j] = v;
   }
@@ -101,8 +124,9 @@ __global__ void __launch_bounds__(kThreads) k_leg_apply(const LegTask* __restric
       for (int j = 0; j < Din; ++j) cfma(acc, a[j], m[j * (kColTile + 1)]);
       const long long q = q0 + qq;
       if (q < rows && kk < kc) {
-        const long long l = q % L, r = q / L;
-        out[l + L * (k0 + kk) + L * (long long)Dout * r] = acc;
+        const uint32_t r = fast_div((uint32_t)q, tk.div_l);
+        const long long l = (long long)((uint32_t)q - r * (uint32_t)L);
+        out[l + L * (k0 + kk) + L * (long long)Dout * (long long)r] = acc;
       }
     }
   }
@@ -357,22 +381,6 @@ static __global__ void k_sum_scaled(const double* __restrict__ x, int n, double 
 //   V'[(v_0,o_0),...,(v_{g-1},o_{g-1}), p'] = sum_p O[o..., p, p'] V[v..., p]
 // merged bond index v + D*o (column-major reshape of (v, o)).
 // ---------------------------------------------------------------------------
-// Division of unsigned values below 2^31 by an invariant divisor d >= 1
-// (Granlund and Montgomery, "Division by invariant integers using
-// multiplication", PLDI 1994): q = (mulhi(x, m) + x) >> s with
-// s = ceil(log2 d) and m = floor(2^32 (2^s - d) / d) + 1, set up once on the
-// host.  mulhi(x, m) < x, so the sum stays below 2^32 for x < 2^31.
-struct FastDiv {
-  uint32_t d, m, s;
-};
-inline FastDiv make_fastdiv(uint32_t d) {
-  uint32_t s = 0;
-  while ((1ull << s) < d) ++s;
-  const unsigned long long m = (((1ull << 32) * ((1ull << s) - d)) / d) + 1;
-  return FastDiv{d, (uint32_t)m, s};
-}
-__device__ __forceinline__ uint32_t fast_div(uint32_t x, const FastDiv& f) { return (__umulhi(x, f.m) + x) >> f.s; }
-
 struct AbsorbTask {
   const void* V;
   void* out;

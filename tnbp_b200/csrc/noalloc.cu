@@ -117,6 +117,7 @@ void message_noalloc(const double* site, const int32_t* shape, int32_t rank, int
     t.out = buf[which];
     t.mat = msgs[k];
     t.L = L; t.R = R; t.Din = shape[k]; t.Dout = shape[k];
+    set_leg_divisors(t);
     t.block_begin = 0;
     legs.push_back(t);
     src = buf[which];
