@@ -30,7 +30,13 @@ inline FastDiv make_fastdiv(uint32_t d) {
   const unsigned long long m = (((1ull << 32) * ((1ull << s) - d)) / d) + 1;
   return FastDiv{d, (uint32_t)m, s};
 }
-__device__ __forceinline__ uint32_t fast_div(uint32_t x, const FastDiv& f) { return (__umulhi(x, f.m) + x) >> f.s; }
+__host__ __device__ __forceinline__ uint32_t fast_div(uint32_t x, const FastDiv& f) {
+#ifdef __CUDA_ARCH__
+  return (__umulhi(x, f.m) + x) >> f.s;
+#else
+  return (uint32_t)((((unsigned long long)x * f.m) >> 32) + x) >> f.s;
+#endif
+}
 
 // ---------------------------------------------------------------------------
 // Leg contraction  out[l, k, r] = sum_j in[l, j, r] * mat[j, k]
