@@ -642,6 +642,13 @@ def run_ours(args, rank, world, local_rank):
                         "hbm_achieved_gbs": (tot_by / n_sw) / ((tot_ms / n_sw) / 1e3) / 1e9 if n_sw else None,
                         "hbm_peak_gbs": peaks.get("hbm_gbs")},
     }
+    # the DRAM bytes the unfused schedule moves per D = 32 sweep (ncu, scaled
+    # from the 5x5 capture) over the measured sweep time: how close the
+    # kernels run to the copy bandwidth on the traffic they must move
+    if traffic and n_sw and peaks.get("hbm_gbs"):
+        rate = traffic / ((tot_ms / n_sw) / 1e3) / 1e9
+        line["roofline"]["schedule_traffic"] = {"gbs": rate, "frac_of_hbm": rate / peaks["hbm_gbs"],
+                                                "traffic_over_algorithmic": traffic / (tot_by / n_sw)}
     if not args.no_fp64:
         # one untimed solve per arm first, as the mixed arm's warm-up: the
         # first BP loop of a shape class on a device runs the wave-budget
