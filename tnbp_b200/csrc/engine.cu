@@ -71,97 +71,9 @@ static void attr_mark(std::vector<char>& flags) {
 }
 
 // ----------------------------------------------------------------- memory
-// Large device buffers that jobs release are kept for the next allocation of
-// (nearly) the same size on the same device, by any stream.  A job's arenas
-// grow step by step as bond dimensions grow, and every solve of a workload
-// repeats the same sizes, but the stream-ordered pool does not always find a
-// freed block for them and then maps fresh memory: on the 16x16 workload
-// that cost 0.1-1.1 s in some solves out of 2.6 s.  A cached block changes
-// hands in stream order (the releasing stream records an event, the
-// allocating stream waits on it).  An allocation the pool cannot serve
-// first returns this device's cached blocks to the pool.
-namespace {
-constexpr size_t kCacheMinBytes = size_t(64) << 20;
-constexpr size_t kCacheMaxBlocks = 32;
-struct CachedBlock {
-  void* p;
-  size_t bytes;
-  int dev;
-  cudaEvent_t ready;
-};
-struct BlockCache {
-  std::mutex mu;
-  std::vector<CachedBlock> blocks;
-};
-BlockCache& block_cache() {
-  static BlockCache* c = new BlockCache();  // blocks live until exit
-  return *c;
-}
-// Frees this device's cached blocks in order on stream s (the caller holds
-// the cache's mutex); true if any was freed.
-bool purge_blocks(BlockCache& C, int dev, cudaStream_t s) {
-  bool any = false;
-  for (size_t i = 0; i < C.blocks.size();) {
-    if (C.blocks[i].dev != dev) { ++i; continue; }
-    cudaStreamWaitEvent(s, C.blocks[i].ready, 0);
-    cudaFreeAsync(C.blocks[i].p, s);
-    cudaEventDestroy(C.blocks[i].ready);
-    C.blocks.erase(C.blocks.begin() + (long)i);
-    any = true;
-  }
-  cudaGetLastError();
-  return any;
-}
-}  // namespace
-
-size_t cached_device_bytes(int dev) {
-  BlockCache& C = block_cache();
-  std::lock_guard<std::mutex> lk(C.mu);
-  size_t b = 0;
-  for (const auto& k : C.blocks)
-    if (k.dev == dev) b += k.bytes;
-  return b;
-}
-
 DevBuf::~DevBuf() { release(); }
 void DevBuf::release() {
   if (p) {
-    // work on the buffer's own device (a job may be released while another
-    // device is current)
-    int cur = -1;
-    const bool switched = dev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != dev &&
-                          cudaSetDevice(dev) == cudaSuccess;
-    struct Restore {
-      bool on;
-      int d;
-      ~Restore() {
-        if (on) cudaSetDevice(d);
-      }
-    } restore{switched, cur};
-    cudaEvent_t ev = nullptr;
-    if (bytes >= kCacheMinBytes && dev >= 0 &&
-        cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess && cudaEventRecord(ev, stream) == cudaSuccess) {
-      BlockCache& C = block_cache();
-      std::lock_guard<std::mutex> lk(C.mu);
-      C.blocks.push_back({p, bytes, dev, ev});
-      size_t mine = 0;
-      for (const auto& k : C.blocks) mine += k.dev == dev;
-      if (mine > kCacheMaxBlocks) {  // the oldest block of this device goes back to the pool
-        for (size_t i = 0; i < C.blocks.size(); ++i) {
-          if (C.blocks[i].dev != dev) continue;
-          cudaStreamWaitEvent(stream, C.blocks[i].ready, 0);
-          cudaFreeAsync(C.blocks[i].p, stream);
-          cudaEventDestroy(C.blocks[i].ready);
-          C.blocks.erase(C.blocks.begin() + (long)i);
-          break;
-        }
-      }
-      p = nullptr;
-      bytes = 0;
-      return;
-    }
-    if (ev) cudaEventDestroy(ev);
-    cudaGetLastError();
     cudaFreeAsync(p, stream);
     p = nullptr;
   }
@@ -170,45 +82,8 @@ void DevBuf::release() {
 void DevBuf::alloc(size_t nbytes, cudaStream_t s) {
   release();
   stream = s;
-  dev = -1;
   if (nbytes == 0) return;
-  const bool have_dev = cudaGetDevice(&dev) == cudaSuccess;
-  if (!have_dev) dev = -1;
-  if (nbytes >= kCacheMinBytes && have_dev) {
-    BlockCache& C = block_cache();
-    std::lock_guard<std::mutex> lk(C.mu);
-    int best = -1;
-    for (size_t i = 0; i < C.blocks.size(); ++i) {
-      const CachedBlock& k = C.blocks[i];
-      if (k.dev != dev || k.bytes < nbytes || k.bytes - nbytes > nbytes / 8) continue;
-      if (best < 0 || k.bytes < C.blocks[(size_t)best].bytes) best = (int)i;
-    }
-    if (best >= 0) {
-      const CachedBlock k = C.blocks[(size_t)best];
-      C.blocks.erase(C.blocks.begin() + best);
-      if (cudaStreamWaitEvent(s, k.ready, 0) == cudaSuccess) {
-        cudaEventDestroy(k.ready);
-        p = k.p;
-        bytes = k.bytes;
-        return;
-      }
-      cudaGetLastError();
-      cudaEventSynchronize(k.ready);
-      cudaEventDestroy(k.ready);
-      cudaFreeAsync(k.p, s);
-    }
-  }
   cudaError_t e = cudaMallocAsync(&p, nbytes, s);
-  if (e != cudaSuccess && have_dev) {
-    cudaGetLastError();
-    BlockCache& C = block_cache();
-    bool freed = false;
-    {
-      std::lock_guard<std::mutex> lk(C.mu);
-      freed = purge_blocks(C, dev, s);
-    }
-    if (freed) e = cudaMallocAsync(&p, nbytes, s);
-  }
   if (e != cudaSuccess) {
     p = nullptr;
     cudaGetLastError();
@@ -657,7 +532,7 @@ size_t device_bytes_available() {
   CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
   CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
   if (reserved > used) fr += (size_t)(reserved - used);
-  return fr + cached_device_bytes(dev);
+  return fr;
 }
 
 size_t Job::scratch_limit() const {

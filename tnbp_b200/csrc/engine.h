@@ -29,7 +29,6 @@ struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
   cudaStream_t stream = nullptr;
-  int dev = -1;  // device the buffer was allocated on
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
@@ -37,7 +36,7 @@ struct DevBuf {
   DevBuf& operator=(DevBuf&& o) noexcept {
     if (this != &o) {
       release();
-      p = o.p; bytes = o.bytes; stream = o.stream; dev = o.dev;
+      p = o.p; bytes = o.bytes; stream = o.stream;
       o.p = nullptr; o.bytes = 0;
     }
     return *this;
